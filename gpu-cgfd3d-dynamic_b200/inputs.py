@@ -1,0 +1,187 @@
+"""Seeded synthetic inputs for the forward dynamic-rupture path.
+
+The reference ships no input files: its examples generate them with MATLAB
+scripts (example/tpv/prep_fault/conf_fault_grid.m: planar fault surface
+x = 0, y = (j - nj/2) dh, z = (k - nk) dh; conf_fault_stress.m: mu_s = 1000
+outside fault_grid, nucleation patch above strength).  These generators
+restate that construction in numpy for the problem sizes this project
+measures on, all in the reference's axes (x fault normal, y strike, z up):
+
+* ``tpv_planar``   -- homogeneous half space, vertical planar fault, flat
+  free surface, CFS-PML (the 160x100x80 case and scaled-down test cases);
+* ``hills_layered`` -- curvilinear grid under Gaussian-hill topography,
+  layered medium with a smoothed random perturbation, vertical fault
+  (the 600x300x240 case the benchmark runs).
+
+Every generator is deterministic for a given seed.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from cgfd import GRID_FAULT_PLANE, GRID_IMPORT, Problem
+
+MPA = 1.0e6
+
+
+def _homog(ni, nj, nk, vp=6000.0, vs=3464.0, rho=2670.0):
+    # md_gen_uniform_el_iso (src/forward/md_t.cu:378-417)
+    mu = np.float32(vs * vs * rho)
+    lam = np.float32(vp * vp * rho - 2.0 * float(mu))
+    shape = (nk, nj, ni)
+    return (np.full(shape, lam, np.float32), np.full(shape, mu, np.float32),
+            np.full(shape, np.float32(rho), np.float32))
+
+
+def _stress(nj, nk, fault_grid, nuc_center, nuc_half, tn=-100.0, ts=60.0, t_nuc=70.0,
+            mu_s=0.65, mu_d=0.50, dc=0.30, c0=0.0, rng=None, ts_field=None):
+    """Initial traction and friction on one fault [nk, nj] (0-based arrays,
+    fault_grid 1-based inclusive like the par file)."""
+    j1, j2, k1, k2 = [v - 1 for v in fault_grid]
+    T0x = np.full((nk, nj), tn * MPA, np.float32)
+    T0y = np.full((nk, nj), ts * MPA, np.float32) if ts_field is None else ts_field.astype(np.float32)
+    T0z = np.zeros((nk, nj), np.float32)
+    jc, kc = nuc_center
+    T0y[kc - nuc_half:kc + nuc_half + 1, jc - nuc_half:jc + nuc_half + 1] = t_nuc * MPA
+    ms = np.full((nk, nj), 1000.0, np.float32)
+    ms[k1:k2 + 1, j1:j2 + 1] = mu_s
+    md = np.full((nk, nj), mu_d, np.float32)
+    Dc = np.full((nk, nj), dc, np.float32)
+    C0 = np.full((nk, nj), c0, np.float32)
+    return T0x, T0y, T0z, ms, md, Dc, C0
+
+
+def tpv_planar(ni=100, nj=160, nk=80, h=200.0, fault_x_index=None, fault_grid=None,
+               nuc_center=None, nuc_half=7, pml=10, dt=0.01, nt=600, nsta=8, seed=1000,
+               margin=40, dynamic_method=2, free_surface=1, mu_s=0.65):
+    """Homogeneous half space with a vertical planar fault.
+
+    Defaults are the 160x100x80 case (h = 200 m, fault at x index 51,
+    fault_grid [21, 141, 21, 80], 15x15-node nucleation patch at 70 MPa
+    centred at strike node 81 and mid-depth of the fault, mu_s 0.65,
+    mu_d 0.50, Dc 0.30 m, 10-layer CFS-PML on five faces, dt 0.01 s,
+    600 steps, 8 surface stations)."""
+    rng = np.random.default_rng(seed)
+    if fault_x_index is None:
+        fault_x_index = ni // 2 + 1
+    if fault_grid is None:
+        fault_grid = [int(round(nj * 0.125)) + 1, int(round(nj * 0.875)) + 1,
+                      int(round(nk * 0.25)) + 1, nk]
+    if nuc_center is None:
+        jc = (fault_grid[0] + fault_grid[1]) // 2 - 1
+        kc = nk - 1 - (nk - fault_grid[2] + 1) // 2
+        nuc_center = (jc, kc)
+    lam, mu, rho = _homog(ni, nj, nk)
+    # conf_fault_grid.m with 1-based j, k
+    jj, kk = np.meshgrid(np.arange(1, nj + 1), np.arange(1, nk + 1))
+    fx = np.zeros((1, nk, nj), np.float32)
+    fy = ((jj - nj / 2.0) * h).astype(np.float32)[None]
+    fz = ((kk - nk) * h).astype(np.float32)[None]
+    st = _stress(nj, nk, fault_grid, nuc_center, nuc_half, mu_s=mu_s)
+    sta_i = rng.integers(pml + 2, ni - pml - 2, nsta)
+    sta_j = rng.integers(pml + 2, nj - pml - 2, nsta)
+    stations = np.stack([sta_i, sta_j, np.full(nsta, nk - 1)], 1).astype(np.float32)
+    fsta = np.array([[nuc_center[0], nuc_center[1]],
+                     [nuc_center[0] + nj // 8, nuc_center[1]],
+                     [nuc_center[0], nk - 1]], np.float32)
+    P = ((pml, pml), (pml, pml), (pml, 0 if free_surface else pml))
+    vp = float(np.sqrt((lam[0, 0, 0] + 2 * mu[0, 0, 0]) / rho[0, 0, 0]))
+    return Problem(ni=ni, nj=nj, nk=nk, dt=dt, lam=lam, mu=mu, rho=rho,
+                   fault_x_index=[fault_x_index], fault_grid=[fault_grid],
+                   T0x=st[0][None], T0y=st[1][None], T0z=st[2][None], mu_s=st[3][None],
+                   mu_d=st[4][None], Dc=st[5][None], C0=st[6][None],
+                   dynamic_method=dynamic_method, welded_margin=margin, free_surface=free_surface,
+                   pml_layers=P, pml_ref_vel=((vp, vp),) * 3,
+                   grid_mode=GRID_FAULT_PLANE, fault_interval=h,
+                   fault_x=fx, fault_y=fy, fault_z=fz,
+                   stations=stations, fault_stations=fsta, max_records=nt + 1,
+                   name=f"tpv_planar_{nj}x{ni}x{nk}")
+
+
+def _smooth(a, n):
+    """Separable box smoothing with periodic wrap, n passes per axis."""
+    out = a.astype(np.float64)
+    for ax in range(out.ndim):
+        for _ in range(n):
+            out = (np.roll(out, 1, ax) + out + np.roll(out, -1, ax)) / 3.0
+    return out
+
+
+def hills_layered(ni=300, nj=600, nk=240, h=100.0, pml=20, seed=1001, nsta=32,
+                  fault_len=400, fault_depth=180, margin=40, dynamic_method=2, nt=3000,
+                  cfl=0.5, nhills=8):
+    """Curvilinear 600x300x240 case (x strike 600, y normal 300, z 240 in the
+    task's axes; here ni = 300 normal, nj = 600 strike, nk = 240 up).
+
+    Topography = sum of ``nhills`` Gaussian hills (amplitude U[100, 800] m,
+    sigma U[2, 6] km); z is stretched linearly from the flat bottom to the
+    surface.  Medium: four layers with Vs 2.0/2.6/3.1/3.6 km/s, Vp = 1.73 Vs,
+    rho = 310 Vp^0.25 (Gardner), times (1 + 0.03 N(0,1)) smoothed.  Vertical
+    fault at the x centre, fault_len x fault_depth nodes below the surface,
+    friction as in ``tpv_planar``; 20-layer PML; dt = cfl * h / (sqrt(3) Vp_max)."""
+    rng = np.random.default_rng(seed)
+    i0 = ni // 2                         # 0-based fault plane
+    xs = (np.arange(ni) - i0) * h
+    ys = (np.arange(nj) - nj / 2.0) * h
+    X2, Y2 = np.meshgrid(xs, ys)         # [nj, ni]
+    topo = np.zeros_like(X2)
+    Lx, Ly = xs[-1] - xs[0], ys[-1] - ys[0]
+    for _ in range(nhills):
+        amp = rng.uniform(100.0, 800.0)
+        sig = rng.uniform(2000.0, 6000.0)
+        cx = rng.uniform(xs[0] + 0.2 * Lx, xs[-1] - 0.2 * Lx)
+        cy = rng.uniform(ys[0] + 0.1 * Ly, ys[-1] - 0.1 * Ly)
+        topo += amp * np.exp(-((X2 - cx) ** 2 + (Y2 - cy) ** 2) / (2 * sig * sig))
+    zb = -(nk - 1) * h
+    t = np.arange(nk) / (nk - 1.0)
+    z3 = zb + (topo[None, :, :] - zb) * t[:, None, None]          # [nk, nj, ni]
+    x3 = np.broadcast_to(X2[None], (nk, nj, ni))
+    y3 = np.broadcast_to(Y2[None], (nk, nj, ni))
+    depth = topo[None] - z3
+    bounds = [0.0, 2000.0, 6000.0, 12000.0]
+    vs_l = [2000.0, 2600.0, 3100.0, 3600.0]
+    vs = np.full(depth.shape, vs_l[0])
+    for b, v in zip(bounds[1:], vs_l[1:]):
+        vs = np.where(depth >= b, v, vs)
+    pert = _smooth(rng.standard_normal((nk, nj, ni)), 3)
+    pert = pert / max(pert.std(), 1e-12)
+    vs = vs * (1.0 + 0.03 * pert)
+    vp = 1.73 * vs
+    rho = 310.0 * vp ** 0.25
+    mu = (vs * vs * rho).astype(np.float32)
+    lam = (vp * vp * rho - 2.0 * vs * vs * rho).astype(np.float32)
+    vp_max = float(vp.max())
+    dt = cfl * h / (math.sqrt(3.0) * vp_max)
+    dt = float(f"{dt:.3g}")
+    jc = nj // 2
+    fault_grid = [jc - fault_len // 2 + 1, jc + fault_len // 2, nk - fault_depth + 1, nk]
+    kc = nk - 1 - fault_depth // 2
+    st = _stress(nj, nk, fault_grid, (jc - 1, kc), 7)
+    sta = np.stack([rng.integers(pml + 4, ni - pml - 4, nsta), rng.integers(pml + 4, nj - pml - 4, nsta),
+                    np.full(nsta, nk - 1)], 1).astype(np.float32)
+    fsta = np.array([[jc - 1, kc], [jc - 1 + 100, kc], [jc - 1, nk - 1]], np.float32)
+    P = ((pml, pml), (pml, pml), (pml, 0))
+    vref = ((vp_max, vp_max),) * 3
+    return Problem(ni=ni, nj=nj, nk=nk, dt=dt, lam=lam, mu=mu, rho=rho.astype(np.float32),
+                   fault_x_index=[i0 + 1], fault_grid=[fault_grid],
+                   T0x=st[0][None], T0y=st[1][None], T0z=st[2][None], mu_s=st[3][None],
+                   mu_d=st[4][None], Dc=st[5][None], C0=st[6][None],
+                   dynamic_method=dynamic_method, welded_margin=margin, free_surface=1,
+                   pml_layers=P, pml_ref_vel=vref, grid_mode=GRID_IMPORT,
+                   x3d=np.ascontiguousarray(x3, np.float32), y3d=np.ascontiguousarray(y3, np.float32),
+                   z3d=np.ascontiguousarray(z3, np.float32),
+                   stations=sta, fault_stations=fsta, max_records=nt + 1,
+                   name=f"hills_layered_{nj}x{ni}x{nk}")
+
+
+def small_planar(seed=7, dynamic_method=2, free_surface=1, pml=5, nt=60, **kw):
+    """A 36x56x32 planar case with a 10-node welded margin: every feature of
+    the path (split nodes reaching the free surface, PML on five faces, both
+    x-operator directions) at a size the CPU oracle runs in seconds."""
+    args = dict(ni=36, nj=56, nk=32, h=200.0, fault_x_index=18, fault_grid=[9, 48, 9, 32],
+                nuc_center=(27, 22), nuc_half=3, pml=pml, dt=0.01, nt=nt, nsta=6, seed=seed,
+                margin=10, dynamic_method=dynamic_method, free_surface=free_surface)
+    args.update(kw)
+    return tpv_planar(**args)

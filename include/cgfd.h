@@ -1,0 +1,208 @@
+/*
+ * cgfd.h -- C ABI of the B200 dynamic-rupture solver (libcgfd.so).
+ *
+ * The reference exposes no library interface: its whole forward path sits
+ * behind one host function,
+ *
+ *   int drv_rk_curv_col_allstep(fd_t*, gd_t*, gd_metric_t*, md_t*, par_t*,
+ *        bdryfree_t*, bdrypml_t*, bdryexp_t*, wav_t*, mympi_t*,
+ *        fault_coef_t*, fault_t*, fault_wav_t*, iorecv_t*, ioline_t*,
+ *        iofault_t*, ioslice_t*, iosnap_t*, io_fault_recv_t*,
+ *        float dt, int nt_total, float t0, char*, char*)
+ *   (src/forward/drv_rk_curv_col.cu:29-52, called from
+ *    src/forward/main_curv_col_el_3d.cu:711)
+ *
+ * preceded by host set-up (grid, metric, medium, PML, fault coefficients;
+ * main_curv_col_el_3d.cu:113-705).  This header replaces both with a
+ * handle: cgfd_create() takes the same inputs as plain host arrays, does the
+ * set-up and copies everything to the GPU once; cgfd_run() advances the
+ * forward time loop; the getters read back the fault fields, the station
+ * seismograms and the wavefield.
+ *
+ * Axes are the reference's: x (index i) is the fault-normal direction, y
+ * (index j) is along strike, z (index k) points up and the free surface is
+ * the top plane k = nk-1.  Every array is C order with x fastest:
+ * 3-D arrays are [nk][nj][ni], fault-plane arrays are [nk][nj].
+ *
+ * Conventions: every call returns CGFD_OK (0) or a negative CGFD_ERR_*
+ * code and never exits the process; cgfd_last_error() returns a message for
+ * the last failing call of the calling thread.  A handle may be used by one
+ * host thread at a time.  The caller owns every pointer it passes; the
+ * library copies what it needs during cgfd_create().
+ */
+#ifndef CGFD_H
+#define CGFD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGFD_ABI_VERSION 1
+
+#define CGFD_MAX_FAULTS 8
+
+/* status codes */
+#define CGFD_OK              0
+#define CGFD_ERR_ARG        -1   /* invalid argument or configuration      */
+#define CGFD_ERR_CUDA       -2   /* CUDA runtime error                     */
+#define CGFD_ERR_NOMEM      -3   /* device or host allocation failed       */
+#define CGFD_ERR_UNSTABLE   -4   /* NaN/Inf found in the wavefield         */
+#define CGFD_ERR_DT         -5   /* dt above the CFL limit of the grid     */
+#define CGFD_ERR_NODEVICE   -6   /* no CUDA device / kernels not loadable  */
+#define CGFD_ERR_STATE      -7   /* call not valid in the handle's state   */
+
+/* grid generation (par key "grid_generation_method") */
+#define CGFD_GRID_FAULT_PLANE 0  /* extrude fault surfaces along x        */
+#define CGFD_GRID_IMPORT      1  /* caller gives all (x,y,z) coordinates  */
+
+/* fault output fields, order of the reference's fault_t.output
+ * (src/forward/fault_info.cu:865-942) */
+#define CGFD_FAULT_TN      0
+#define CGFD_FAULT_TS1     1
+#define CGFD_FAULT_TS2     2
+#define CGFD_FAULT_VS      3
+#define CGFD_FAULT_VS1     4
+#define CGFD_FAULT_VS2     5
+#define CGFD_FAULT_SLIP    6
+#define CGFD_FAULT_SLIP1   7
+#define CGFD_FAULT_SLIP2   8
+#define CGFD_FAULT_PEAK_VS 9
+#define CGFD_FAULT_INIT_T0 10
+#define CGFD_FAULT_NFIELD  11
+
+/* wavefield components, order of the reference's wav_t
+ * (src/forward/wav_t.cu:57-108) */
+#define CGFD_VX  0
+#define CGFD_VY  1
+#define CGFD_VZ  2
+#define CGFD_TXX 3
+#define CGFD_TYY 4
+#define CGFD_TZZ 5
+#define CGFD_TYZ 6
+#define CGFD_TXZ 7
+#define CGFD_TXY 8
+#define CGFD_NCMP 9
+
+typedef struct cgfd_config {
+  /* interior grid points ("number_of_total_grid_points_{x,y,z}") */
+  int ni, nj, nk;
+  /* time step ("size_of_time_step"); checked against the CFL limit
+   * (CFL 1.3, src/forward/fd_t.cu:57) unless check_stability == 0 */
+  float dt;
+  int check_stability;
+  /* "dynamic_method": 1 (continuity matrices) or 2 (traction rate) */
+  int dynamic_method;
+  /* faults: constant-x planes; indices are 1-based as in the par file */
+  int num_faults;
+  int fault_x_index[CGFD_MAX_FAULTS];     /* "fault_x_index"           */
+  int fault_grid[CGFD_MAX_FAULTS][4];     /* "fault_grid" j1,j2,k1,k2  */
+  /* nodes closer than this to the y sides (and to the bottom, or to the
+   * top without free surface) are welded; the reference hard-codes 40
+   * (src/forward/fault_info.cu:1044-1060) */
+  int welded_margin;
+  /* 1: traction-image free surface on the top face ("boundary_z_top":
+   * {"free": ...}) */
+  int free_surface;
+  /* CFS-PML per face [dim x,y,z][side left/bottom, right/top]; 0 layers =
+   * no PML ("boundary_*": {"cfspml": {...}}) */
+  int   pml_layers[3][2];
+  float pml_alpha_max[3][2];
+  float pml_beta_max[3][2];
+  float pml_ref_vel[3][2];
+  /* geometry */
+  int grid_mode;                 /* CGFD_GRID_FAULT_PLANE / CGFD_GRID_IMPORT */
+  float fault_interval;          /* "fault_inteval": x spacing (FAULT_PLANE) */
+  const float *fault_x, *fault_y, *fault_z;   /* [num_faults][nk][nj]        */
+  const float *x3d, *y3d, *z3d;               /* [nk][nj][ni] (GRID_IMPORT)   */
+  /* isotropic elastic medium, [nk][nj][ni] */
+  const float *lambda, *mu, *rho;
+  /* fault initial traction and friction ("init_stress_<id>.nc"),
+   * [num_faults][nk][nj] */
+  const float *T0x, *T0y, *T0z, *mu_s, *mu_d, *Dc, *C0;
+  /* volume stations: 0-based global interior grid index (i, j, k),
+   * fractional parts interpolate; [num_stations][3] */
+  int num_stations;
+  const float *station_ijk;
+  /* fault stations: fault id (0-based) and 0-based (j, k) on the fault
+   * plane, fractional parts interpolate; [num_fault_stations] and [..][2] */
+  int num_fault_stations;
+  const int   *fault_station_fault;
+  const float *fault_station_jk;
+  /* capacity of the station/fault-station time series (records) */
+  int max_records;
+} cgfd_config;
+
+typedef struct cgfd_solver cgfd_solver;
+
+/* ABI version compiled into the library (CGFD_ABI_VERSION). */
+int cgfd_abi_version(void);
+
+/* Fill cfg with the reference's defaults (welded margin 40, dynamic
+ * method 2, stability check on, no PML, free surface off). */
+void cgfd_config_default(cgfd_config *cfg);
+
+/* Set up grid, metric, medium, PML and fault coefficients on the host and
+ * move the problem to the current CUDA device.
+ * Replaces main_curv_col_el_3d.cu:113-705 + the device set-up at
+ * drv_rk_curv_col.cu:90-100. */
+int cgfd_create(const cgfd_config *cfg, cgfd_solver **out);
+
+/* Advance nsteps time steps (4 RK stages each); before each step the
+ * stations and fault stations are sampled, as io_recv_keep /
+ * io_fault_recv_keep do at drv_rk_curv_col.cu:215-218.
+ * Replaces the time loop of drv_rk_curv_col.cu:209-636. */
+int cgfd_run(cgfd_solver *s, int nsteps);
+
+/* Number of steps taken so far. */
+int cgfd_steps_done(const cgfd_solver *s, int *it);
+
+/* Dense grid spacing bound: largest dt that passes the stability check. */
+int cgfd_dt_max(const cgfd_solver *s, float *dtmax);
+
+/* One fault field (CGFD_FAULT_*) of fault `fault_id` (0-based), interior
+ * nodes, [nk][nj].  The data behind io_fault_nc_put
+ * (src/forward/io_funcs.cu:2027-2099). */
+int cgfd_get_fault(cgfd_solver *s, int fault_id, int field, float *out);
+
+/* All 11 fault fields of one fault at once, [11][nk][nj]. */
+int cgfd_get_fault_all(cgfd_solver *s, int fault_id, float *out);
+
+/* Station seismograms [num_stations][9][nrec], nrec = records taken so
+ * far (*nrec set on return, <= max_records). */
+int cgfd_get_stations(cgfd_solver *s, float *out, int *nrec);
+
+/* Fault-station time series [num_fault_stations][9][nrec] of
+ * Tn,Ts1,Ts2,Vs,Vs1,Vs2,Slip,Slip1,Slip2. */
+int cgfd_get_fault_stations(cgfd_solver *s, float *out, int *nrec);
+
+/* One wavefield component (CGFD_VX..CGFD_TXY) of the current level at
+ * interior points, [nk][nj][ni]. */
+int cgfd_get_wavefield(cgfd_solver *s, int cmp, float *out);
+
+/* Overwrite one component of the current level at interior points (ghosts
+ * stay zero), [nk][nj][ni].  For initial conditions and tests; the
+ * reference always starts from rest (alloc.cu:543-551). */
+int cgfd_set_wavefield(cgfd_solver *s, int cmp, const float *in);
+
+/* Size in bytes of a checkpoint of the full solver state. */
+int cgfd_checkpoint_size(cgfd_solver *s, unsigned long long *bytes);
+/* Copy the full time-stepping state (wavefield, PML auxiliaries, fault
+ * wavefield and fault state, step counter) to host memory `buf`. */
+int cgfd_checkpoint(cgfd_solver *s, void *buf, unsigned long long bytes);
+/* Restore a state written by cgfd_checkpoint on a solver created from the
+ * same configuration. */
+int cgfd_restore(cgfd_solver *s, const void *buf, unsigned long long bytes);
+
+/* Kernel launches issued by the last cgfd_run call (for accounting). */
+int cgfd_last_launches(const cgfd_solver *s, long long *launches);
+
+/* Release device and host memory of the handle. */
+void cgfd_destroy(cgfd_solver *s);
+
+/* Message of the last error of the calling thread ("" if none). */
+const char *cgfd_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGFD_H */
