@@ -1,0 +1,64 @@
+"""Build libcgfd.so (sm_100a) in-tree: gpu-cgfd3d-dynamic_b200/lib/libcgfd.so.
+
+nvcc cross-compiles for sm_100a without a GPU; the host set-up is g++ with
+OpenMP.  Objects go to gpu-cgfd3d-dynamic_b200/_build/.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIBDIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIBDIR, "libcgfd.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+
+CU = ["volume.cu", "fault.cu", "api.cu"]
+CPP = ["setup.cpp"]
+HEADERS = ["common.h", "ops.cuh", "setup.h"]
+
+
+def _newer(dst, srcs):
+    if not os.path.exists(dst):
+        return True
+    t = os.path.getmtime(dst)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def build(verbose=False, ptxas_info=False):
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "cgfd.h")]
+    objs = []
+    for f in CPP:
+        src, obj = os.path.join(CSRC, f), os.path.join(BUILD, f + ".o")
+        if _newer(obj, [src] + hdrs):
+            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.check_call(cmd)
+        objs.append(obj)
+    for f in CU:
+        src, obj = os.path.join(CSRC, f), os.path.join(BUILD, f + ".o")
+        if _newer(obj, [src] + hdrs) or ptxas_info:
+            cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                                   "--expt-relaxed-constexpr", "-c", src, "-o", obj]
+            if ptxas_info:
+                cmd += ["-Xptxas", "-v"]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.check_call(cmd)
+        objs.append(obj)
+    if _newer(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, ptxas_info="-v" in sys.argv))

@@ -1,0 +1,478 @@
+// api.cu -- the C ABI of include/cgfd.h.
+//
+// cgfd_create runs the host set-up (setup.cpp), allocates the device state
+// and copies the problem once.  cgfd_run replays one CUDA graph per time
+// step; there are eight graphs, one per MacCormack operator pair
+// (it % 8, src/forward/drv_rk_curv_col.cu:237), each holding the station
+// sample, 4 x (fault-plane kernels + fused volume kernel) and the step
+// counter advance.  Time levels P and E swap by step parity, which it % 8
+// fixes, so the graphs never need their arguments updated.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cgfd.h"
+#include "ops.cuh"
+#include "setup.h"
+
+namespace cgfd {
+void launch_volume(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_fault_stage(const FaultArgs &a, cudaStream_t st);
+void launch_record(const StationArgs &a, cudaStream_t st);
+void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
+}  // namespace cgfd
+
+using namespace cgfd;
+
+namespace {
+
+thread_local std::string g_err;
+int fail(int code, const std::string &m) { g_err = m; return code; }
+
+// FD_Flags (src/forward/fd_t.cu:146-159): 0 backward, 1 forward
+const int kPairs[8][3] = { {0,0,0},{1,1,0},{1,1,1},{0,0,1},{0,1,0},{1,0,0},{1,0,1},{0,1,1} };
+const float kRkA[3] = { 0.5f, 0.5f, 1.0f };
+const float kRkB[4] = { 1.0f / 6.0f, 1.0f / 3.0f, 1.0f / 3.0f, 1.0f / 6.0f };
+
+struct FaultState {
+  FaultDev d;
+  int j0 = 0, k0 = 0, nj = 0, nk = 0;   // bounding box of split nodes (interior)
+  float *lev[4] = {};                   // storage slots, [9][2][ny*nz]
+  uint8_t *flag = nullptr;
+  float *mat = nullptr, *fmat = nullptr, *scal = nullptr, *out = nullptr;
+};
+
+struct PmlState {
+  PmlFaceDev d{};
+  float *coef = nullptr;                // A | B | D
+  float *aux[4] = {};
+};
+
+}  // namespace
+
+struct cgfd_solver {
+  Grid g{};
+  int imethod = 2, isfree = 0;
+  float dt = 0.f, dtmax = 0.f;
+  float *w[4] = {};                     // storage slots of the 4 levels
+  float *met = nullptr, *med = nullptr, *free_mat = nullptr;
+  PmlState pml[6];
+  std::vector<FaultState> faults;
+  StationDev st{};
+  long *sta_idx = nullptr;
+  float *sta_w = nullptr, *fsta_w = nullptr;
+  int *fsta_fid = nullptr, *fsta_idx = nullptr;
+  float *seis = nullptr, *fseis = nullptr;
+  Ctl *ctl = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph[8] = {};
+  bool use_graph = true;
+  int it = 0;
+  long long launches_per_step = 0, last_launches = 0;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+template <class T>
+cudaError_t dalloc(cgfd_solver *s, T **p, size_t n) {
+  cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+  if (e == cudaSuccess) { s->allocs.push_back(*p); e = cudaMemsetAsync(*p, 0, std::max<size_t>(n, 1) * sizeof(T), s->stream); }
+  return e;
+}
+
+// storage slot of logical level L (0 P, 1 A, 2 B, 3 E) at step parity
+int slot(int L, int it) {
+  if (L == LA || L == LB) return L;
+  const bool odd = (it & 1) != 0;
+  return (L == LP) != odd ? 0 : 3;
+}
+
+void destroy(cgfd_solver *s) {
+  if (!s) return;
+  for (int q = 0; q < 8; q++) if (s->graph[q]) cudaGraphExecDestroy(s->graph[q]);
+  for (void *p : s->allocs) cudaFree(p);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+// enqueue one time step (graph capture or direct launches)
+void enqueue_step(cgfd_solver *s, int it) {
+  const int ip = it % 8;
+  long long nl = 0;
+  StationArgs sa{};
+  sa.g = s->g; sa.st = s->st; sa.w = s->w[slot(LP, it)]; sa.ns = (long)s->g.ny * s->g.nz; sa.ctl = s->ctl;
+  for (size_t f = 0; f < s->faults.size(); f++) sa.fout[f] = s->faults[f].out;
+  if ((s->st.n + s->st.nf) > 0 && s->st.max_rec > 0) { launch_record(sa, s->stream); nl++; }
+  for (int stage = 0; stage < 4; stage++) {
+    const int idir = (kPairs[ip][0] + stage) % 2, jdir = (kPairs[ip][1] + stage) % 2, kdir = (kPairs[ip][2] + stage) % 2;
+    const int mode = stage == 0 ? RK_FIRST : (stage == 3 ? RK_LAST : RK_MID);
+    const int Lcur = stage == 0 ? LP : (stage == 2 ? LB : LA);
+    const int Lout = stage == 0 ? LA : (stage == 1 ? LB : (stage == 2 ? LA : -1));
+    const float ca = stage < 3 ? kRkA[stage] * s->dt : 0.f, cb = kRkB[stage] * s->dt;
+    const int scur = slot(Lcur, it), spre = slot(LP, it), send = slot(LE, it);
+    const int sout = Lout >= 0 ? slot(Lout, it) : -1;
+    for (auto &F : s->faults) {
+      FaultArgs a{};
+      a.g = s->g; a.F = F.d;
+      a.wcur = s->w[scur]; a.wpre = s->w[spre]; a.wout = sout >= 0 ? s->w[sout] : nullptr; a.wend = s->w[send];
+      a.met = s->met; a.med = s->med; a.free_mat = s->free_mat;
+      a.fc = F.lev[scur]; a.fp = F.lev[spre]; a.fo = sout >= 0 ? F.lev[sout] : nullptr; a.fe = F.lev[send];
+      a.idir = idir; a.jdir = jdir; a.kdir = kdir; a.mode = mode;
+      a.ca = ca; a.cb = cb; a.rkb = kRkB[stage]; a.dt = s->dt;
+      a.isfree = s->isfree; a.imethod = s->imethod;
+      a.j0 = F.j0; a.k0 = F.k0; a.nj = F.nj; a.nk = F.nk; a.ctl = s->ctl;
+      launch_fault_stage(a, s->stream);
+      nl += (F.nj > 0 && F.nk > 0) ? 3 : 1;
+    }
+    VolArgs v{};
+    v.g = s->g; v.cur = s->w[scur]; v.pre = s->w[spre]; v.out = sout >= 0 ? s->w[sout] : nullptr; v.end = s->w[send];
+    v.met = s->met; v.med = s->med; v.free_mat = s->free_mat;
+    v.ca = ca; v.cb = cb; v.isfree = s->isfree;
+    v.nfault = (int)s->faults.size();
+    for (size_t f = 0; f < s->faults.size(); f++) { v.fi0[f] = s->faults[f].d.i0; v.fflag[f] = s->faults[f].flag; }
+    for (int q = 0; q < 6; q++) {
+      v.pml[q] = s->pml[q].d;
+      if (!v.pml[q].on) continue;
+      v.pml[q].acur = s->pml[q].aux[scur]; v.pml[q].apre = s->pml[q].aux[spre];
+      v.pml[q].aout = sout >= 0 ? s->pml[q].aux[sout] : nullptr; v.pml[q].aend = s->pml[q].aux[send];
+    }
+    launch_volume(v, idir, jdir, kdir, mode, s->stream);
+    nl++;
+  }
+  launch_advance(s->ctl, s->st.max_rec, s->stream);
+  nl++;
+  s->launches_per_step = nl;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(e == cudaErrorMemoryAllocation ? CGFD_ERR_NOMEM : CGFD_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+extern "C" {
+
+int cgfd_abi_version(void) { return CGFD_ABI_VERSION; }
+
+void cgfd_config_default(cgfd_config *c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->check_stability = 1;
+  c->dynamic_method = 2;
+  c->welded_margin = 40;
+  c->grid_mode = CGFD_GRID_FAULT_PLANE;
+  for (int d = 0; d < 3; d++) for (int s = 0; s < 2; s++) {
+    c->pml_alpha_max[d][s] = 3.14f; c->pml_beta_max[d][s] = 2.0f; c->pml_ref_vel[d][s] = 6000.f;
+  }
+}
+
+const char *cgfd_last_error(void) { return g_err.c_str(); }
+
+int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
+  if (!cfg || !out) return fail(CGFD_ERR_ARG, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CGFD_ERR_NODEVICE, "no CUDA device visible");
+  }
+  HostSetup H;
+  std::string msg;
+  int rc = build_setup(cfg, H, msg);
+  if (rc != CGFD_OK) return fail(rc, msg);
+
+  cgfd_solver *s = new cgfd_solver();
+  cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { destroy(s); return cuda_fail(e, "stream"); }
+  s->g = H.g; s->imethod = H.imethod; s->isfree = H.isfree; s->dt = H.dt; s->dtmax = H.dtmax;
+  const char *ng = std::getenv("CGFD_NO_GRAPH");
+  s->use_graph = !(ng && ng[0] == '1');
+  const Grid &g = s->g;
+  const size_t lev = (size_t)NCMP * g.scmp, ns = (size_t)g.ny * g.nz;
+#define CK(x, what) do { cudaError_t _e = (x); if (_e != cudaSuccess) { destroy(s); return cuda_fail(_e, what); } } while (0)
+  for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
+  CK(dalloc(s, &s->met, H.metric.size()), "metric");
+  CK(dalloc(s, &s->med, H.media.size()), "medium");
+  CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
+  CK(cudaMemcpyAsync(s->met, H.metric.data(), H.metric.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy metric");
+  CK(cudaMemcpyAsync(s->med, H.media.data(), H.media.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy medium");
+  CK(cudaMemcpyAsync(s->free_mat, H.free_mat.data(), H.free_mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy free");
+  for (int d = 0; d < 3; d++) for (int sd = 0; sd < 2; sd++) {
+    const PmlHost &P = H.pml[d][sd];
+    PmlState &S = s->pml[2 * d + sd];
+    S.d.on = P.on; S.d.d = d; S.d.s = sd; S.d.L = P.L;
+    if (!P.on) continue;
+    S.d.i1 = P.i1; S.d.j1 = P.j1; S.d.k1 = P.k1;
+    S.d.fni = P.i2 - P.i1 + 1; S.d.fnj = P.j2 - P.j1 + 1; S.d.fnk = P.k2 - P.k1 + 1;
+    S.d.siz = (long)S.d.fni * S.d.fnj * S.d.fnk;
+    const int np = P.L + 1;
+    CK(dalloc(s, &S.coef, 3 * (size_t)np), "pml coef");
+    std::vector<float> cf(3 * np);
+    std::copy(P.A.begin(), P.A.end(), cf.begin());
+    std::copy(P.B.begin(), P.B.end(), cf.begin() + np);
+    std::copy(P.D.begin(), P.D.end(), cf.begin() + 2 * np);
+    CK(cudaMemcpyAsync(S.coef, cf.data(), cf.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy pml");
+    S.d.A = S.coef; S.d.B = S.coef + np; S.d.D = S.coef + 2 * np;
+    for (int L = 0; L < 4; L++) CK(dalloc(s, &S.aux[L], (size_t)NCMP * S.d.siz), "pml aux");
+  }
+  for (size_t f = 0; f < H.faults.size(); f++) {
+    const FaultHost &Fh = H.faults[f];
+    FaultState F;
+    for (int L = 0; L < 4; L++) CK(dalloc(s, &F.lev[L], 18 * ns), "fault wavefield");
+    CK(dalloc(s, &F.flag, ns), "fault flags");
+    CK(dalloc(s, &F.mat, Fh.mat.size()), "fault matrices");
+    CK(dalloc(s, &F.fmat, Fh.fmat.size()), "fault free matrices");
+    CK(dalloc(s, &F.scal, Fh.scal.size()), "fault scalars");
+    CK(dalloc(s, &F.out, Fh.out.size()), "fault output");
+    CK(cudaMemcpyAsync(F.flag, Fh.flag.data(), ns, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(cudaMemcpyAsync(F.mat, Fh.mat.data(), Fh.mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(cudaMemcpyAsync(F.fmat, Fh.fmat.data(), Fh.fmat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(cudaMemcpyAsync(F.scal, Fh.scal.data(), Fh.scal.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(cudaMemcpyAsync(F.out, Fh.out.data(), Fh.out.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    F.d.i0 = Fh.i0; F.d.bit = 1 << f; F.d.flag_in = F.flag; F.d.flag = F.flag;
+    F.d.mat = F.mat; F.d.fmat = F.fmat; F.d.scal = F.scal; F.d.out = F.out;
+    int j0 = g.nj, j1 = -1, k0 = g.nk, k1 = -1;
+    for (int k = 0; k < g.nk; k++) for (int j = 0; j < g.nj; j++)
+      if (Fh.flag[(size_t)(j + NG) + (size_t)(k + NG) * g.ny] & FL_SPLIT) {
+        j0 = std::min(j0, j); j1 = std::max(j1, j); k0 = std::min(k0, k); k1 = std::max(k1, k);
+      }
+    if (j1 >= 0) { F.j0 = j0; F.k0 = k0; F.nj = j1 - j0 + 1; F.nk = k1 - k0 + 1; }
+    s->faults.push_back(F);
+  }
+  // stations
+  StationDev &st = s->st;
+  st.n = (int)(H.sta_w.size() / 3); st.nf = (int)H.fsta_fid.size(); st.max_rec = H.max_rec;
+  CK(dalloc(s, &s->sta_idx, H.sta_idx.size()), "stations");
+  CK(dalloc(s, &s->sta_w, H.sta_w.size()), "stations");
+  CK(dalloc(s, &s->fsta_fid, H.fsta_fid.size()), "stations");
+  CK(dalloc(s, &s->fsta_idx, H.fsta_idx.size()), "stations");
+  CK(dalloc(s, &s->fsta_w, H.fsta_w.size()), "stations");
+  CK(dalloc(s, &s->seis, (size_t)st.n * 9 * std::max(1, st.max_rec)), "seismograms");
+  CK(dalloc(s, &s->fseis, (size_t)st.nf * 9 * std::max(1, st.max_rec)), "fault seismograms");
+  if (!H.sta_idx.empty()) {
+    CK(cudaMemcpyAsync(s->sta_idx, H.sta_idx.data(), H.sta_idx.size() * sizeof(long), cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(cudaMemcpyAsync(s->sta_w, H.sta_w.data(), H.sta_w.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+  }
+  if (!H.fsta_fid.empty()) {
+    CK(cudaMemcpyAsync(s->fsta_fid, H.fsta_fid.data(), H.fsta_fid.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(cudaMemcpyAsync(s->fsta_idx, H.fsta_idx.data(), H.fsta_idx.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(cudaMemcpyAsync(s->fsta_w, H.fsta_w.data(), H.fsta_w.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+  }
+  st.idx = s->sta_idx; st.w = s->sta_w; st.fid = s->fsta_fid; st.fidx = s->fsta_idx; st.fw = s->fsta_w;
+  st.seis = s->seis; st.fseis = s->fseis;
+  CK(dalloc(s, &s->ctl, 1), "control block");
+  CK(cudaStreamSynchronize(s->stream), "set-up");
+#undef CK
+  *out = s;
+  return CGFD_OK;
+}
+
+int cgfd_run(cgfd_solver *s, int nsteps) {
+  if (!s || nsteps < 0) return fail(CGFD_ERR_ARG, "bad argument");
+  long long nl = 0;
+  for (int q = 0; q < nsteps; q++) {
+    const int it = s->it;
+    if (s->use_graph) {
+      cudaGraphExec_t &G = s->graph[it % 8];
+      if (!G) {
+        cudaGraph_t gr;
+        cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_fail(e, "begin capture");
+        enqueue_step(s, it);
+        e = cudaStreamEndCapture(s->stream, &gr);
+        if (e != cudaSuccess) return cuda_fail(e, "end capture");
+        e = cudaGraphInstantiate(&G, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) { G = nullptr; return cuda_fail(e, "instantiate"); }
+      }
+      cudaError_t e = cudaGraphLaunch(G, s->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "graph launch");
+    } else {
+      enqueue_step(s, it);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "launch");
+    }
+    nl += s->launches_per_step;
+    s->it++;
+  }
+  s->last_launches = nl;
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "run");
+  Ctl c;
+  e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "read control block");
+  if (c.it != s->it) return fail(CGFD_ERR_STATE, "device step counter out of step with the host");
+  if (c.err & 1) return fail(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
+  return CGFD_OK;
+}
+
+int cgfd_steps_done(const cgfd_solver *s, int *it) {
+  if (!s || !it) return fail(CGFD_ERR_ARG, "bad argument");
+  *it = s->it;
+  return CGFD_OK;
+}
+
+int cgfd_dt_max(const cgfd_solver *s, float *d) {
+  if (!s || !d) return fail(CGFD_ERR_ARG, "bad argument");
+  *d = s->dtmax;
+  return CGFD_OK;
+}
+
+int cgfd_get_fault_all(cgfd_solver *s, int f, float *out) {
+  if (!s || !out || f < 0 || f >= (int)s->faults.size()) return fail(CGFD_ERR_ARG, "bad argument");
+  const Grid &g = s->g;
+  const size_t ns = (size_t)g.ny * g.nz;
+  std::vector<float> h((size_t)CGFD_FAULT_NFIELD * ns);
+  cudaError_t e = cudaMemcpyAsync(h.data(), s->faults[f].out, h.size() * 4, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "read fault");
+  for (int q = 0; q < CGFD_FAULT_NFIELD; q++)
+    for (int k = 0; k < g.nk; k++)
+      std::memcpy(out + ((size_t)q * g.nk + k) * g.nj, h.data() + q * ns + (size_t)(k + NG) * g.ny + NG, (size_t)g.nj * 4);
+  return CGFD_OK;
+}
+
+int cgfd_get_fault(cgfd_solver *s, int f, int field, float *out) {
+  if (!s || !out || f < 0 || f >= (int)s->faults.size() || field < 0 || field >= CGFD_FAULT_NFIELD)
+    return fail(CGFD_ERR_ARG, "bad argument");
+  const Grid &g = s->g;
+  const size_t ns = (size_t)g.ny * g.nz;
+  std::vector<float> h(ns);
+  cudaError_t e = cudaMemcpyAsync(h.data(), s->faults[f].out + field * ns, ns * 4, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "read fault");
+  for (int k = 0; k < g.nk; k++) std::memcpy(out + (size_t)k * g.nj, h.data() + (size_t)(k + NG) * g.ny + NG, (size_t)g.nj * 4);
+  return CGFD_OK;
+}
+
+static int get_series(cgfd_solver *s, float *dev, int n, float *out, int *nrec) {
+  Ctl c;
+  cudaError_t e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "read control block");
+  if (nrec) *nrec = c.nrec;
+  if (!out || n == 0 || c.nrec == 0) return CGFD_OK;
+  const int mr = s->st.max_rec;
+  std::vector<float> h((size_t)n * 9 * mr);
+  e = cudaMemcpy(h.data(), dev, h.size() * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "read series");
+  for (size_t q = 0; q < (size_t)n * 9; q++) std::memcpy(out + q * c.nrec, h.data() + q * mr, (size_t)c.nrec * 4);
+  return CGFD_OK;
+}
+
+int cgfd_get_stations(cgfd_solver *s, float *out, int *nrec) {
+  if (!s) return fail(CGFD_ERR_ARG, "bad argument");
+  return get_series(s, s->seis, s->st.n, out, nrec);
+}
+
+int cgfd_get_fault_stations(cgfd_solver *s, float *out, int *nrec) {
+  if (!s) return fail(CGFD_ERR_ARG, "bad argument");
+  return get_series(s, s->fseis, s->st.nf, out, nrec);
+}
+
+int cgfd_get_wavefield(cgfd_solver *s, int cmp, float *out) {
+  if (!s || !out || cmp < 0 || cmp >= NCMP) return fail(CGFD_ERR_ARG, "bad argument");
+  const Grid &g = s->g;
+  std::vector<float> h(g.scmp);
+  cudaError_t e = cudaMemcpyAsync(h.data(), s->w[slot(LP, s->it)] + (size_t)cmp * g.scmp, g.scmp * 4, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "read wavefield");
+  for (int k = 0; k < g.nk; k++) for (int j = 0; j < g.nj; j++)
+    std::memcpy(out + ((size_t)k * g.nj + j) * g.ni, h.data() + g.at(NG, j + NG, k + NG), (size_t)g.ni * 4);
+  return CGFD_OK;
+}
+
+int cgfd_set_wavefield(cgfd_solver *s, int cmp, const float *in) {
+  if (!s || !in || cmp < 0 || cmp >= NCMP) return fail(CGFD_ERR_ARG, "bad argument");
+  const Grid &g = s->g;
+  std::vector<float> h(g.scmp);
+  float *dst = s->w[slot(LP, s->it)] + (size_t)cmp * g.scmp;
+  cudaError_t e = cudaMemcpy(h.data(), dst, g.scmp * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "read wavefield");
+  for (int k = 0; k < g.nk; k++) for (int j = 0; j < g.nj; j++)
+    std::memcpy(h.data() + g.at(NG, j + NG, k + NG), in + ((size_t)k * g.nj + j) * g.ni, (size_t)g.ni * 4);
+  e = cudaMemcpy(dst, h.data(), g.scmp * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "write wavefield");
+  return CGFD_OK;
+}
+
+// checkpoint: [Ctl][P level][PML P levels][per fault: P level, scal, out, flag][seis][fseis]
+static std::vector<std::pair<void *, size_t>> state_parts(cgfd_solver *s) {
+  std::vector<std::pair<void *, size_t>> v;
+  const Grid &g = s->g;
+  const size_t ns = (size_t)g.ny * g.nz;
+  const int sp = slot(LP, s->it);
+  v.push_back({ s->ctl, sizeof(Ctl) });
+  v.push_back({ s->w[sp], (size_t)NCMP * g.scmp * 4 });
+  for (int q = 0; q < 6; q++) if (s->pml[q].d.on) v.push_back({ s->pml[q].aux[sp], (size_t)NCMP * s->pml[q].d.siz * 4 });
+  for (auto &F : s->faults) {
+    v.push_back({ F.lev[sp], 18 * ns * 4 });
+    v.push_back({ F.scal, (size_t)NFS * ns * 4 });
+    v.push_back({ F.out, (size_t)CGFD_FAULT_NFIELD * ns * 4 });
+    v.push_back({ F.flag, ns });
+  }
+  v.push_back({ s->seis, (size_t)s->st.n * 9 * std::max(1, s->st.max_rec) * 4 });
+  v.push_back({ s->fseis, (size_t)s->st.nf * 9 * std::max(1, s->st.max_rec) * 4 });
+  return v;
+}
+
+int cgfd_checkpoint_size(cgfd_solver *s, unsigned long long *bytes) {
+  if (!s || !bytes) return fail(CGFD_ERR_ARG, "bad argument");
+  unsigned long long n = sizeof(int);
+  for (auto &p : state_parts(s)) n += p.second;
+  *bytes = n;
+  return CGFD_OK;
+}
+
+int cgfd_checkpoint(cgfd_solver *s, void *buf, unsigned long long bytes) {
+  unsigned long long need = 0;
+  int rc = cgfd_checkpoint_size(s, &need);
+  if (rc) return rc;
+  if (!buf || bytes < need) return fail(CGFD_ERR_ARG, "checkpoint buffer too small");
+  char *p = (char *)buf;
+  std::memcpy(p, &s->it, sizeof(int));
+  p += sizeof(int);
+  for (auto &q : state_parts(s)) {
+    cudaError_t e = cudaMemcpy(p, q.first, q.second, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "checkpoint");
+    p += q.second;
+  }
+  return CGFD_OK;
+}
+
+int cgfd_restore(cgfd_solver *s, const void *buf, unsigned long long bytes) {
+  unsigned long long need = 0;
+  int rc = cgfd_checkpoint_size(s, &need);
+  if (rc) return rc;
+  if (!buf || bytes != need) return fail(CGFD_ERR_ARG, "checkpoint size does not match this solver");
+  const char *p = (const char *)buf;
+  int it;
+  std::memcpy(&it, p, sizeof(int));
+  p += sizeof(int);
+  if (it < 0) return fail(CGFD_ERR_ARG, "corrupt checkpoint");
+  s->it = it;   // sets the level parity before the parts are placed
+  for (auto &q : state_parts(s)) {
+    cudaError_t e = cudaMemcpy(q.first, p, q.second, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "restore");
+    p += q.second;
+  }
+  return CGFD_OK;
+}
+
+int cgfd_last_launches(const cgfd_solver *s, long long *n) {
+  if (!s || !n) return fail(CGFD_ERR_ARG, "bad argument");
+  *n = s->last_launches;
+  return CGFD_OK;
+}
+
+void cgfd_destroy(cgfd_solver *s) {
+  if (s) cudaStreamSynchronize(s->stream);
+  destroy(s);
+}
+
+}  // extern "C"

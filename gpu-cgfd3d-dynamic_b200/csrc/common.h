@@ -1,0 +1,118 @@
+// common.h -- data layout and device argument blocks shared by the host
+// set-up (setup.cpp), the kernels (volume.cu, fault.cu) and the C ABI
+// (api.cu).
+//
+// HBM layout.  Every 3-D field is stored like the reference's (3 ghost
+// points per side, x fastest, src/forward/gd_t.cu:2124-2140) but with a
+// padded row pitch: index p = (i + XOFF) + j*sy + k*sz for ghost-inclusive
+// indices (i, j, k), sy a multiple of 32 floats.  XOFF = 1 puts the first
+// interior point (i = 3) on a 16-byte boundary.  A wavefield level is 9
+// components of scmp floats (Vx,Vy,Vz,Txx,Tyy,Tzz,Tyz,Txz,Txy); four levels
+// P (time n), A and B (ping-pong stage inputs) and E (time n+1 accumulator)
+// replace the reference's pre/tmp/rhs/end, because each fused stage writes
+// its output level directly instead of a separate rhs array.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define CGFD_HD __host__ __device__
+#else
+#define CGFD_HD
+#endif
+
+namespace cgfd {
+
+constexpr int NG = 3;            // ghost points per side
+constexpr int XOFF = 1;          // x offset for 16-byte alignment of interior rows
+constexpr int NCMP = 9;
+constexpr int MAXF = 8;          // faults
+
+enum Cmp { VX = 0, VY, VZ, TXX, TYY, TZZ, TYZ, TXZ, TXY };
+// fault wavefield components [side][comp] (src/forward/fault_wav_t.cu:96-150)
+enum FCmp { FVX = 0, FVY, FVZ, FT2X, FT2Y, FT2Z, FT3X, FT3Y, FT3Z };
+// metric component order in the metric block
+enum Met { MJAC = 0, MXIX, MXIY, MXIZ, METX, METY, METZ, MZTX, MZTY, MZTZ };
+
+// per-node 3x3 fault matrices, [NFM][nodes][9]
+enum FaultMat {
+  FM_D21_1 = 0, FM_D22_1, FM_D23_1, FM_D31_1, FM_D32_1, FM_D33_1,
+  FM_D21_2, FM_D22_2, FM_D23_2, FM_D31_2, FM_D32_2, FM_D33_2,
+  FM_M2P1, FM_M2P2, FM_M2P3, FM_M2P4, FM_M2P5,
+  FM_P2M1, FM_P2M2, FM_P2M3, FM_P2M4, FM_P2M5,
+  FM_T1VXMIN, FM_VYVXMIN, FM_VZVXMIN, FM_T1VXPLUS, FM_VYVXPLUS, FM_VZVXPLUS,
+  NFM
+};
+// per-strike-column free-surface fault matrices, [NFF][ny][9]
+enum FaultFreeMat {
+  FF_VX2VZ1 = 0, FF_VY2VZ1, FF_VX2VZ2, FF_VY2VZ2,
+  FF_P2M1, FF_P2M2, FF_P2M3, FF_M2P1, FF_M2P2, FF_M2P3,
+  FF_T1VXMIN, FF_VYVXMIN, FF_T1VXPLUS, FF_VYVXPLUS,
+  NFF
+};
+// per-node scalar fault data, [NFS][nodes]
+enum FaultScal {
+  FS_T0X = 0, FS_T0Y, FS_T0Z, FS_MUS, FS_MUD, FS_DC, FS_C0,
+  FS_RHO0, FS_RHO1,                 // rho on the minus / plus side
+  FS_S1X, FS_S1Y, FS_S1Z, FS_S2X, FS_S2Y, FS_S2Z,
+  FS_TTN, FS_TTS1, FS_TTS2,         // stage traction (not stored; kept for layout)
+  FS_T1X, FS_T1Y, FS_T1Z,           // traction at the split node of this stage
+  FS_HT1X, FS_HT1Y, FS_HT1Z,        // dT1/dt of the last step
+  FS_MT1X, FS_MT1Y, FS_MT1Z,        // T1 of the last step
+  NFS
+};
+// fault node flags (uint8 bits)
+enum FaultFlag { FL_SPLIT = 1, FL_RUPY = 2, FL_RUPZ = 4, FL_GRID = 8, FL_T0SET = 16, FL_RUP = 32 };
+
+struct Grid {
+  int ni, nj, nk;        // interior points
+  int nx, ny, nz;        // with ghosts
+  long sy, sz;           // strides of j and k (elements)
+  long scmp;             // elements per component (sz * nz)
+  CGFD_HD long at(int i, int j, int k) const { return (long)(i + XOFF) + (long)j * sy + (long)k * sz; }
+};
+
+struct PmlFaceDev {
+  int on, d, s, L;
+  int i1, j1, k1;        // first point of the face region (ghost-inclusive indices)
+  int fni, fnj, fnk;     // face region extents
+  long siz;              // fni*fnj*fnk
+  const float *A, *B, *D;   // per layer along the normal
+  // auxiliary-field levels used by one stage (9*siz floats each): stage
+  // input, time-n level, next-stage output, end accumulator
+  const float *acur, *apre;
+  float *aout, *aend;
+};
+
+struct FaultDev {
+  int i0;                   // ghost-inclusive x index of the fault plane
+  int bit;
+  const uint8_t *flag_in;   // FL_SPLIT / FL_RUPY / FL_RUPZ / FL_GRID per node [ny*nz]
+  uint8_t *flag;            // mutable flags (FL_T0SET, FL_RUP)
+  const float *mat;         // [NFM][ny*nz][9]
+  const float *fmat;        // [NFF][ny][9]
+  float *scal;              // [NFS][ny*nz]
+  float *out;               // [11][ny*nz] Tn..Init_t0
+};
+
+struct StationDev {
+  int n, nf, max_rec;
+  const long *idx;          // [n][8] volume indices (corner 4 unused: reference quirk)
+  const float *w;           // [n][3] di, dj, dk
+  const int *fid;           // [nf] fault id
+  const int *fidx;          // [nf][4] node indices
+  const float *fw;          // [nf][2] dj, dk
+  float *seis;              // [n][9][max_rec]
+  float *fseis;             // [nf][9][max_rec]
+};
+
+// control block in device memory, advanced on the device so that a step
+// can be replayed as a CUDA graph
+struct Ctl {
+  int it;                   // steps taken
+  int nrec;                 // records taken
+  int err;                  // bit 0: non-finite value seen
+  int pad;
+};
+
+}  // namespace cgfd

@@ -1,0 +1,586 @@
+// fault.cu -- split-node fault kernels, one thread per fault node.
+//
+// Per RK stage the reference launches, per fault, wave2fault, the trial
+// traction + slip-weakening friction kernel, fault2wave, the fault velocity
+// RHS, the fault stress RHS (forward or backward variant), two fault RK
+// updates, fault2wave again and the stage traction update, each as its own
+// kernel (src/forward/drv_rk_curv_col.cu:277-588).  Here that becomes three
+// kernels over the fault plane:
+//
+//   k_fault_weld    welded nodes: fault wavefield from the volume at i0
+//                   (wave2fault_gpu, src/forward/transform.cu:101-212)
+//   k_fault_vel     split nodes: T1 traction image, trial traction and
+//                   linear slip-weakening friction (trial_slipweakening_gpu,
+//                   src/forward/trial_slipweakening.cu:92-388), velocity RHS
+//                   at i0-3..i0+3 and at both split nodes
+//                   (sv_curv_col_el_iso_rhs_fault_velo_gpu,
+//                   src/forward/sv_curv_col_el_iso_fault_gpu.cu:192-429),
+//                   RK update of those velocities, stage traction output
+//                   (fault_var_stage_update_gpu, fault_wav_t.cu:291-316)
+//   k_fault_stress  split nodes: stress RHS at i0-3..i0+3 and fault traction
+//                   rates (..._stress_F_gpu :432-1159 / _B_gpu :1162-1879),
+//                   RK update, then the split-node volume point from the
+//                   fault fields (fault2wave_gpu, transform.cu:293-376) and,
+//                   after the last stage, slip / slip rate / rupture time
+//                   (fault_var_update_gpu, fault_wav_t.cu:198-264)
+//
+// The volume stage kernel skips i0-3..i0+3 of split nodes, so these kernels
+// own those points' RK update.  Fault-plane work is a few percent of a step.
+#include <cuda_runtime.h>
+
+#include "ops.cuh"
+
+namespace cgfd {
+
+namespace {
+
+__device__ __forceinline__ long fidx(int c, int m, long ns, long nd) { return ((long)c * 2 + m) * ns + nd; }
+
+// J * (e_ax . sigma) at point q, 3 components
+__device__ __forceinline__ void trac3(const float *__restrict__ w, const float *__restrict__ met, long sc,
+                                      long q, int ax, float t[3]) {
+  const float J = __ldg(met + MJAC * sc + q);
+  const float ex = __ldg(met + ax * sc + q), ey = __ldg(met + (ax + 1) * sc + q), ez = __ldg(met + (ax + 2) * sc + q);
+  const float sxx = __ldg(w + TXX * sc + q), syy = __ldg(w + TYY * sc + q), szz = __ldg(w + TZZ * sc + q);
+  const float syz = __ldg(w + TYZ * sc + q), sxz = __ldg(w + TXZ * sc + q), sxy = __ldg(w + TXY * sc + q);
+  t[0] = J * (ex * sxx + ey * sxy + ez * sxz);
+  t[1] = J * (ex * sxy + ey * syy + ez * syz);
+  t[2] = J * (ex * sxz + ey * syz + ez * szz);
+}
+
+// stage update of one value: first stage (out, end from the input), middle
+// stages (out from P, end accumulates), last stage (end accumulates)
+__device__ __forceinline__ void rk_put(int mode, float ca, float cb, const float *cur, const float *pre,
+                                       float *out, float *end, long o, float h) {
+  if (mode == RK_FIRST) {
+    const float v = cur[o];
+    out[o] = v + ca * h;
+    end[o] = v + cb * h;
+  } else if (mode == RK_MID) {
+    out[o] = pre[o] + ca * h;
+    end[o] += cb * h;
+  } else {
+    end[o] += cb * h;
+  }
+}
+
+// split-node volume point from the fault fields (fault2wave_gpu,
+// transform.cu:293-376): velocity = mean of the two sides, stress from the
+// traction vectors [T1 | mean T2 | mean T3] through the inverse metric.
+__device__ void split_to_volume(const Grid &g, const float *__restrict__ met, long sc, long ns, long nd,
+                                int i0, int J, int K, const float *f, const float T1[3], float *wt) {
+  const long p0 = g.at(i0, J, K);
+  float mt[3][3];   // columns e_xi, e_eta, e_zeta
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) mt[r][c] = __ldg(met + (1 + 3 * c + r) * sc + p0);
+  const float rj = 1.0f / __ldg(met + MJAC * sc + p0);
+  float tr[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    tr[r][0] = T1[r];
+    tr[r][1] = (f[fidx(FT2X + r, 0, ns, nd)] + f[fidx(FT2X + r, 1, ns, nd)]) * 0.5f;
+    tr[r][2] = (f[fidx(FT3X + r, 0, ns, nd)] + f[fidx(FT3X + r, 1, ns, nd)]) * 0.5f;
+  }
+  const float c00 = mt[1][1] * mt[2][2] - mt[2][1] * mt[1][2], c01 = mt[2][1] * mt[0][2] - mt[0][1] * mt[2][2];
+  const float c02 = mt[0][1] * mt[1][2] - mt[0][2] * mt[1][1], c10 = mt[1][2] * mt[2][0] - mt[1][0] * mt[2][2];
+  const float c11 = mt[0][0] * mt[2][2] - mt[2][0] * mt[0][2], c12 = mt[1][0] * mt[0][2] - mt[0][0] * mt[1][2];
+  const float c20 = mt[1][0] * mt[2][1] - mt[1][1] * mt[2][0], c21 = mt[2][0] * mt[0][1] - mt[0][0] * mt[2][1];
+  const float c22 = mt[0][0] * mt[1][1] - mt[0][1] * mt[1][0];
+  const float id = 1.0f / (c00 * mt[0][0] + c01 * mt[1][0] + c02 * mt[2][0]);
+  const float mi[3][3] = { { c00 * id, c01 * id, c02 * id }, { c10 * id, c11 * id, c12 * id }, { c20 * id, c21 * id, c22 * id } };
+  float st[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) st[r][c] = (tr[r][0] * mi[0][c] + tr[r][1] * mi[1][c] + tr[r][2] * mi[2][c]) * rj;
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    wt[(VX + c) * sc + p0] = (f[fidx(FVX + c, 0, ns, nd)] + f[fidx(FVX + c, 1, ns, nd)]) * 0.5f;
+  wt[TXX * sc + p0] = st[0][0];
+  wt[TYY * sc + p0] = st[1][1];
+  wt[TZZ * sc + p0] = st[2][2];
+  wt[TXY * sc + p0] = (st[0][1] + st[1][0]) * 0.5f;
+  // the reference's fault2wave_gpu receives Tyz and Txz in swapped
+  // positions (transform.cu:281-289 vs :293-300); kept for parity
+  wt[TYZ * sc + p0] = (st[0][2] + st[2][0]) * 0.5f;
+  wt[TXZ * sc + p0] = (st[1][2] + st[2][1]) * 0.5f;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+__global__ void k_fault_weld(const FaultArgs a) {
+  const Grid &g = a.g;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= g.nj || k >= g.nk) return;
+  const int J = j + NG, K = k + NG;
+  const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny, sc = g.scmp;
+  if (a.F.flag[nd] & FL_SPLIT) return;
+  const long p = g.at(a.F.i0, J, K);
+  const float *w = a.wcur;
+  float t2[3], t3[3];
+  trac3(w, a.met, sc, p, METX, t2);
+  trac3(w, a.met, sc, p, MZTX, t3);
+  float *f = const_cast<float *>(a.fc);
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      f[fidx(FVX + c, m, ns, nd)] = w[(VX + c) * sc + p];
+      f[fidx(FT2X + c, m, ns, nd)] = t2[c];
+      f[fidx(FT3X + c, m, ns, nd)] = t3[c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_fault_vel(const FaultArgs a) {
+  const Grid &g = a.g;
+  const int j = a.j0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = a.k0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= a.j0 + a.nj || k >= a.k0 + a.nk) return;
+  const int J = j + NG, K = k + NG;
+  const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny, sc = g.scmp;
+  const FaultDev &F = a.F;
+  const uint8_t fl = F.flag[nd];
+  if (!(fl & FL_SPLIT)) return;
+  const int i0 = F.i0;
+  const float *w = a.wcur, *met = a.met;
+  const long ny = g.ny;
+  const int km = g.nk - (k + 1);
+  const bool surf = a.isfree && km <= 3;
+  const int nf = km + 3;
+
+  // T1 = J e_xi . sigma along x through the split node, i0-6..i0+6 (index 6
+  // is the split node, filled after the friction law)
+  float X1[13][3];
+#pragma unroll
+  for (int l = -6; l <= 6; l++) {
+    if (l == 0) continue;
+    trac3(w, met, sc, g.at(i0 + l, J, K), MXIX, X1[l + 6]);
+  }
+
+  // along-fault derivatives of the fault tractions, both sides
+  float DyT2[2][3], DzT3[2][3], R[2][3];
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float *t2 = a.fc + fidx(FT2X + c, m, ns, nd);
+      DyT2[m][c] = (fl & FL_RUPY) ? mac22(t2, 1, a.jdir) : drp_rt(t2, 1, a.jdir);
+      const float *t3 = a.fc + fidx(FT3X + c, m, ns, nd);
+      float dz;
+      if (surf) {
+        // traction image of T3 about the free surface
+        float v[7];
+#pragma unroll
+        for (int l = 0; l < 7; l++) v[l] = __ldg(t3 + (long)(l - 3) * ny);
+        v[nf] = 0.f;
+        for (int l = nf + 1; l < 7; l++) v[l] = -v[2 * nf - l];
+        dz = drp_v(v + 3, a.kdir);
+      } else {
+        dz = (fl & FL_RUPZ) ? mac22(t3, ny, a.kdir) : drp_rt(t3, ny, a.kdir);
+      }
+      DzT3[m][c] = dz;
+      const int s = 2 * m - 1;
+      const float img = kA1 * X1[6 + s][c] + kA2 * X1[6 + 2 * s][c] + kA3 * X1[6 + 3 * s][c];
+      R[m][c] = 0.5f * ((float)s * img + (DyT2[m][c] + DzT3[m][c]));
+    }
+  }
+
+  // trial traction from the velocity jump of time level n and friction
+  const long p0 = g.at(i0, J, K);
+  const float jac0 = __ldg(met + MJAC * sc + p0);
+  const float rho0 = F.scal[FS_RHO0 * ns + nd], rho1 = F.scal[FS_RHO1 * ns + nd];
+  const float M0 = 0.5f * jac0 * rho0, M1 = 0.5f * jac0 * rho1;
+  float Tr[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float dV = a.fp[fidx(FVX + c, 1, ns, nd)] - a.fp[fidx(FVX + c, 0, ns, nd)];
+    Tr[c] = 2.0f * (M0 * M1 * dV / a.dt + M0 * R[1][c] - M1 * R[0][c]) / (kA0 * (M0 + M1));
+  }
+  float vn[3] = { __ldg(met + MXIX * sc + p0), __ldg(met + MXIY * sc + p0), __ldg(met + MXIZ * sc + p0) };
+  const float vn0 = sqrtf(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
+  const float jacvec = jac0 * vn0;
+  vn[0] /= vn0; vn[1] /= vn0; vn[2] /= vn0;
+  const float T0[3] = { F.scal[FS_T0X * ns + nd], F.scal[FS_T0Y * ns + nd], F.scal[FS_T0Z * ns + nd] };
+  float Tl[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) Tl[c] = Tr[c] / jacvec + T0[c];
+  const float Tn0 = Tl[0] * vn[0] + Tl[1] * vn[1] + Tl[2] * vn[2];
+  float Ts[3] = { Tl[0] - vn[0] * Tn0, Tl[1] - vn[1] * Tn0, Tl[2] - vn[2] * Tn0 };
+  const float Ts0 = sqrtf(Ts[0] * Ts[0] + Ts[1] * Ts[1] + Ts[2] * Ts[2]);
+  bool change = false;
+  float Tau_n = Tn0;
+  if (Tn0 >= 0.f) { Tau_n = 0.f; change = true; }     // the fault cannot open
+  const float slip = F.out[CGFD_FAULT_SLIP * ns + nd];
+  const float mus = F.scal[FS_MUS * ns + nd], mud = F.scal[FS_MUD * ns + nd];
+  const float Dc = F.scal[FS_DC * ns + nd], C0 = F.scal[FS_C0 * ns + nd];
+  const float fr = slip <= Dc ? mus - (mus - mud) * slip / Dc : mud;
+  const float Tau_c = -fr * Tau_n + C0;
+  float Tau_s = Ts0;
+  if (Ts0 >= Tau_c) { Tau_s = Tau_c; change = true; }
+  float Tau[3], T1s[3];
+  if (change) {
+    const float q = fabsf(Ts0) < 1e-1f ? 0.f : Tau_s / Ts0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) { Tau[c] = Tau_n * vn[c] + q * Ts[c]; T1s[c] = (Tau[c] - T0[c]) * jacvec; }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; c++) { Tau[c] = Tl[c]; T1s[c] = Tr[c]; }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) { F.scal[(FS_T1X + c) * ns + nd] = T1s[c]; X1[6][c] = T1s[c]; }
+  // the stage input level sees the new split-node traction before the volume
+  // kernel reads it (drv_rk_curv_col.cu:285, fault2wave on w_cur); this
+  // kernel never reads the volume at i0 itself
+  split_to_volume(g, met, sc, ns, nd, i0, J, K, a.fc, T1s, const_cast<float *>(a.wcur));
+  {
+    const float s1[3] = { F.scal[FS_S1X * ns + nd], F.scal[FS_S1Y * ns + nd], F.scal[FS_S1Z * ns + nd] };
+    const float s2[3] = { F.scal[FS_S2X * ns + nd], F.scal[FS_S2Y * ns + nd], F.scal[FS_S2Z * ns + nd] };
+    const float tTs1 = Tau[0] * s1[0] + Tau[1] * s1[1] + Tau[2] * s1[2];
+    const float tTs2 = Tau[0] * s2[0] + Tau[1] * s2[1] + Tau[2] * s2[2];
+    float *Tn = F.out + CGFD_FAULT_TN * ns + nd, *T1o = F.out + CGFD_FAULT_TS1 * ns + nd, *T2o = F.out + CGFD_FAULT_TS2 * ns + nd;
+    if (a.mode == RK_FIRST) { *Tn = a.rkb * Tau_n; *T1o = a.rkb * tTs1; *T2o = a.rkb * tTs2; }
+    else { *Tn += a.rkb * Tau_n; *T1o += a.rkb * tTs1; *T2o += a.rkb * tTs2; }
+  }
+
+  // velocity RHS at i0+s, s = -3..3 (s != 0)
+#pragma unroll
+  for (int s = -3; s <= 3; s++) {
+    if (s == 0) continue;
+    const long q = g.at(i0 + s, J, K);
+    float hv[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float v1[7];
+#pragma unroll
+      for (int l = 0; l < 7; l++) v1[l] = X1[6 + s + l - 3][c];
+      // odd extension of T1 through the split node (Zhang's traction image)
+      if (s == -2) { v1[6] = 2.f * v1[5] - v1[4]; }
+      if (s == -1) { v1[5] = 2.f * v1[4] - v1[3]; v1[6] = 2.f * v1[4] - v1[2]; }
+      if (s == 1) { v1[0] = 2.f * v1[2] - v1[4]; v1[1] = 2.f * v1[2] - v1[3]; }
+      if (s == 2) { v1[0] = 2.f * v1[1] - v1[2]; }
+      hv[c] = drp_v(v1 + 3, a.idir);
+    }
+    float v2[7][3], v3[7][3];
+#pragma unroll
+    for (int l = 0; l < 7; l++) {
+      trac3(w, met, sc, q + (long)(l - 3) * g.sy, METX, v2[l]);
+      trac3(w, met, sc, q + (long)(l - 3) * g.sz, MZTX, v3[l]);
+    }
+    const float rr = __ldg(a.med + 2 * sc + q) / __ldg(met + MJAC * sc + q);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float y[7], z[7];
+#pragma unroll
+      for (int l = 0; l < 7; l++) { y[l] = v2[l][c]; z[l] = v3[l][c]; }
+      if (surf) {
+        z[nf] = 0.f;
+        for (int l = nf + 1; l < 7; l++) z[l] = -z[2 * nf - l];
+      }
+      const float h = (hv[c] + drp_v(y + 3, a.jdir) + drp_v(z + 3, a.kdir)) * rr;
+      rk_put(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, (VX + c) * sc + q, h);
+    }
+  }
+
+  // split-node velocity RHS and RK update
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const float rr = 1.0f / ((m ? rho1 : rho0) * jac0);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float dx = m == 0 ? (kA0 * X1[6][c] - kA1 * X1[5][c] - kA2 * X1[4][c] - kA3 * X1[3][c])
+                              : (-kA0 * X1[6][c] + kA1 * X1[7][c] + kA2 * X1[8][c] + kA3 * X1[9][c]);
+      const float h = (dx + DyT2[m][c] + DzT3[m][c]) * rr;
+      rk_put(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, fidx(FVX + c, m, ns, nd), h);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_fault_stress(const FaultArgs a) {
+  const Grid &g = a.g;
+  const int j = a.j0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = a.k0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= a.j0 + a.nj || k >= a.k0 + a.nk) return;
+  const int J = j + NG, K = k + NG;
+  const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny, sc = g.scmp;
+  const FaultDev &F = a.F;
+  const uint8_t fl = F.flag[nd];
+  if (!(fl & FL_SPLIT)) return;
+  const int i0 = F.i0;
+  const float *w = a.wcur, *met = a.met;
+  const long ny = g.ny, sy = g.sy, sz = g.sz;
+  const int km = g.nk - (k + 1);
+  const bool fwd = a.idir == 1;
+
+  // split nodes: along-fault velocity derivatives of each side
+  float Sx[2][3], Sy[2][3], Sz[2][3];
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float *v = a.fc + fidx(FVX + c, m, ns, nd);
+      Sy[m][c] = (fl & FL_RUPY) ? mac22(v, 1, a.jdir) : drp_rt(v, 1, a.jdir);
+      if (a.isfree && km == 1) Sz[m][c] = mac22(v, ny, a.kdir);
+      else if (a.isfree && km == 2) Sz[m][c] = mac24(v, ny, a.kdir);
+      else Sz[m][c] = (fl & FL_RUPZ) ? mac22(v, ny, a.kdir) : drp_rt(v, ny, a.kdir);
+    }
+  }
+  const float *fv[3] = { a.fc + fidx(FVX, 0, ns, nd), a.fc + fidx(FVY, 0, ns, nd), a.fc + fidx(FVZ, 0, ns, nd) };
+  // velocity on each side of the fault from the volume: fV[m][c]
+  float fV[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) { fV[0][c] = fv[c][0]; fV[1][c] = fv[c][ns]; }
+
+  const float *mat = F.mat;
+  auto M = [&](int id) { return mat + ((long)id * ns + nd) * 9; };
+  const bool top = a.isfree && km == 0;
+  if (!top) {
+    if (a.imethod == 1) {
+      // one side from its one-sided difference, the other from continuity
+      // of traction rate across the fault
+      float o1[3], o2[3], o3[3], o4[3], o5[3];
+      if (fwd) {
+        const long q = g.at(i0 + 1, J, K);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[1][c] = w[(VX + c) * sc + q] - fV[1][c];
+        mv3(M(FM_P2M1), Sx[1], o1); mv3(M(FM_P2M2), Sy[1], o2); mv3(M(FM_P2M3), Sz[1], o3);
+        mv3(M(FM_P2M4), Sy[0], o4); mv3(M(FM_P2M5), Sz[0], o5);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[0][c] = o1[c] + o2[c] + o3[c] - o4[c] - o5[c];
+      } else {
+        const long q = g.at(i0 - 1, J, K);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[0][c] = fV[0][c] - w[(VX + c) * sc + q];
+        mv3(M(FM_M2P1), Sx[0], o1); mv3(M(FM_M2P2), Sy[0], o2); mv3(M(FM_M2P3), Sz[0], o3);
+        mv3(M(FM_M2P4), Sy[1], o4); mv3(M(FM_M2P5), Sz[1], o5);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[1][c] = o1[c] + o2[c] + o3[c] - o4[c] - o5[c];
+      }
+    } else {
+      // normal derivative of each side from the traction rate
+      float dt1[3] = { 0.f, 0.f, 0.f };
+      if (fl & FL_GRID) { dt1[0] = F.scal[FS_HT1X * ns + nd]; dt1[1] = F.scal[FS_HT1Y * ns + nd]; dt1[2] = F.scal[FS_HT1Z * ns + nd]; }
+      float o1[3], o2[3], o3[3];
+      mv3(M(FM_T1VXPLUS), dt1, o1); mv3(M(FM_VYVXPLUS), Sy[1], o2); mv3(M(FM_VZVXPLUS), Sz[1], o3);
+#pragma unroll
+      for (int c = 0; c < 3; c++) Sx[1][c] = o1[c] - o2[c] - o3[c];
+      mv3(M(FM_T1VXMIN), dt1, o1); mv3(M(FM_VYVXMIN), Sy[0], o2); mv3(M(FM_VZVXMIN), Sz[0], o3);
+#pragma unroll
+      for (int c = 0; c < 3; c++) Sx[0][c] = o1[c] - o2[c] - o3[c];
+    }
+  } else {
+    // split nodes on the free surface: traction-free top as well
+    auto FM = [&](int id) { return F.fmat + ((long)id * ny + J) * 9; };
+    float o1[3], o2[3], o3[3];
+    if (a.imethod == 1) {
+      if (fwd) {
+        const long q = g.at(i0 + 1, J, K);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[1][c] = w[(VX + c) * sc + q] - fV[1][c];
+        mv3(FM(FF_P2M1), Sx[1], o1); mv3(FM(FF_P2M2), Sy[1], o2); mv3(FM(FF_P2M3), Sy[0], o3);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[0][c] = o1[c] + o2[c] - o3[c];
+      } else {
+        const long q = g.at(i0 - 1, J, K);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[0][c] = fV[0][c] - w[(VX + c) * sc + q];
+        mv3(FM(FF_M2P1), Sx[0], o1); mv3(FM(FF_M2P2), Sy[0], o2); mv3(FM(FF_M2P3), Sy[1], o3);
+#pragma unroll
+        for (int c = 0; c < 3; c++) Sx[1][c] = o1[c] + o2[c] - o3[c];
+      }
+    } else {
+      float dt1[3] = { 0.f, 0.f, 0.f };
+      if (fl & FL_GRID) { dt1[0] = F.scal[FS_HT1X * ns + nd]; dt1[1] = F.scal[FS_HT1Y * ns + nd]; dt1[2] = F.scal[FS_HT1Z * ns + nd]; }
+      mv3(FM(FF_T1VXPLUS), dt1, o1); mv3(FM(FF_VYVXPLUS), Sy[1], o2);
+#pragma unroll
+      for (int c = 0; c < 3; c++) Sx[1][c] = o1[c] - o2[c];
+      mv3(FM(FF_T1VXMIN), dt1, o1); mv3(FM(FF_VYVXMIN), Sy[0], o2);
+#pragma unroll
+      for (int c = 0; c < 3; c++) Sx[0][c] = o1[c] - o2[c];
+    }
+    mv3(FM(FF_VX2VZ2), Sx[1], o1); mv3(FM(FF_VY2VZ2), Sy[1], o2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) Sz[1][c] = o1[c] + o2[c];
+    mv3(FM(FF_VX2VZ1), Sx[0], o1); mv3(FM(FF_VY2VZ1), Sy[0], o2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) Sz[0][c] = o1[c] + o2[c];
+  }
+
+  // fault traction rates and RK update of T2, T3 on both sides
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const int b2 = m ? FM_D21_2 : FM_D21_1, b3 = m ? FM_D31_2 : FM_D31_1;
+    float g1[3], g2[3], g3[3];
+    mv3(M(b2), Sx[m], g1); mv3(M(b2 + 1), Sy[m], g2); mv3(M(b2 + 2), Sz[m], g3);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      rk_put(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, fidx(FT2X + c, m, ns, nd), g1[c] + g2[c] + g3[c]);
+    mv3(M(b3), Sx[m], g1); mv3(M(b3 + 1), Sy[m], g2); mv3(M(b3 + 2), Sz[m], g3);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      rk_put(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, fidx(FT3X + c, m, ns, nd), g1[c] + g2[c] + g3[c]);
+  }
+
+  // stress RHS at the six volume points i0+s, s = -3..3 (s != 0)
+#pragma unroll
+  for (int s = -3; s <= 3; s++) {
+    if (s == 0) continue;
+    const long q = g.at(i0 + s, J, K);
+    float dx[3], dy[3], dz[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float *v = w + (VX + c) * sc + q;
+      const float f = fV[s < 0 ? 0 : 1][c];
+      if (fwd) {
+        // forward operators; points left of the fault see the minus side
+        if (s == 3) dx[c] = drp<1>(v, 1);
+        else if (s == 2) dx[c] = mac24(v, 1, 1);
+        else if (s == 1) dx[c] = mac22(v, 1, 1);
+        else if (s == -1) dx[c] = f - __ldg(v);
+        else if (s == -2) dx[c] = kB1 * __ldg(v) + kB2 * __ldg(v + 1) + kB3 * f;
+        else dx[c] = kC1 * __ldg(v - 1) + kC2 * __ldg(v) + kC3 * __ldg(v + 1) + kC4 * __ldg(v + 2) + kC5 * f;
+      } else {
+        if (s == -3) dx[c] = drp<0>(v, 1);
+        else if (s == -2) dx[c] = mac24(v, 1, 0);
+        else if (s == -1) dx[c] = mac22(v, 1, 0);
+        else if (s == 1) dx[c] = __ldg(v) - f;
+        else if (s == 2) dx[c] = -(kB3 * f + kB2 * __ldg(v - 1) + kB1 * __ldg(v));
+        else dx[c] = -(kC5 * f + kC4 * __ldg(v - 2) + kC3 * __ldg(v - 1) + kC2 * __ldg(v) + kC1 * __ldg(v + 1));
+      }
+      dy[c] = drp_rt(v, sy, a.jdir);
+      if (a.isfree && km == 1) dz[c] = mac22(v, sz, a.kdir);
+      else if (a.isfree && km == 2) dz[c] = mac24(v, sz, a.kdir);
+      else dz[c] = drp_rt(v, sz, a.kdir);
+    }
+    if (top) {
+      const float *X = a.free_mat + ((long)J * g.nx + (i0 + s)) * 9;
+      const float *Y = X + (long)g.ny * g.nx * 9;
+      float o1[3], o2[3];
+      mv3(X, dx, o1); mv3(Y, dy, o2);
+#pragma unroll
+      for (int c = 0; c < 3; c++) dz[c] = o1[c] + o2[c];
+    }
+    float e[3][3];
+#pragma unroll
+    for (int r = 0; r < 9; r++) e[r / 3][r % 3] = __ldg(met + (1 + r) * sc + q);
+    const float lam = __ldg(a.med + q), mu = __ldg(a.med + sc + q);
+    const float l2m = lam + 2.0f * mu;
+    float G[3][3];
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) G[c][b] = e[0][b] * dx[c] + e[1][b] * dy[c] + e[2][b] * dz[c];
+    float h[6];
+    h[0] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]);
+    h[1] = l2m * G[1][1] + lam * (G[0][0] + G[2][2]);
+    h[2] = l2m * G[2][2] + lam * (G[0][0] + G[1][1]);
+    h[3] = mu * (G[1][2] + G[2][1]);   // Tyz
+    h[4] = mu * (G[0][2] + G[2][0]);   // Txz
+    h[5] = mu * (G[0][1] + G[1][0]);   // Txy
+#pragma unroll
+    for (int c = 0; c < 6; c++) rk_put(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, (TXX + c) * sc + q, h[c]);
+  }
+
+  // the split-node volume point of the output level from the fault fields
+  {
+    const bool last = a.mode == RK_LAST;
+    const float T1s[3] = { F.scal[FS_T1X * ns + nd], F.scal[FS_T1Y * ns + nd], F.scal[FS_T1Z * ns + nd] };
+    split_to_volume(g, met, sc, ns, nd, i0, J, K, last ? a.fe : a.fo, T1s, last ? a.wend : a.wout);
+  }
+
+  // end of step: slip rate, slip, traction rate, peak slip rate, rupture time
+  if (a.mode == RK_LAST) {
+    const float *f = a.fe;
+    const float s1[3] = { F.scal[FS_S1X * ns + nd], F.scal[FS_S1Y * ns + nd], F.scal[FS_S1Z * ns + nd] };
+    const float s2[3] = { F.scal[FS_S2X * ns + nd], F.scal[FS_S2Y * ns + nd], F.scal[FS_S2Z * ns + nd] };
+    float dV[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) dV[c] = f[fidx(FVX + c, 1, ns, nd)] - f[fidx(FVX + c, 0, ns, nd)];
+    const float Vs1 = dV[0] * s1[0] + dV[1] * s1[1] + dV[2] * s1[2];
+    const float Vs2 = dV[0] * s2[0] + dV[1] * s2[1] + dV[2] * s2[2];
+    const float Vs = sqrtf(Vs2 * Vs2 + Vs1 * Vs1);
+    float *o = F.out;
+    o[CGFD_FAULT_VS * ns + nd] = Vs;
+    o[CGFD_FAULT_VS1 * ns + nd] = Vs1;
+    o[CGFD_FAULT_VS2 * ns + nd] = Vs2;
+    o[CGFD_FAULT_SLIP * ns + nd] += Vs * a.dt;
+    o[CGFD_FAULT_SLIP1 * ns + nd] += Vs1 * a.dt;
+    o[CGFD_FAULT_SLIP2 * ns + nd] += Vs2 * a.dt;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float t1 = F.scal[(FS_T1X + c) * ns + nd];
+      F.scal[(FS_HT1X + c) * ns + nd] = (t1 - F.scal[(FS_MT1X + c) * ns + nd]) / a.dt;
+      F.scal[(FS_MT1X + c) * ns + nd] = t1;
+    }
+    if (Vs > o[CGFD_FAULT_PEAK_VS * ns + nd]) o[CGFD_FAULT_PEAK_VS * ns + nd] = Vs;
+    uint8_t fl2 = F.flag[nd];
+    if (!(fl2 & FL_T0SET) && Vs > 1e-3f) {
+      o[CGFD_FAULT_INIT_T0 * ns + nd] = (a.ctl->it + 1) * a.dt;
+      F.flag[nd] = fl2 | FL_T0SET;
+    }
+    if (!isfinite(Vs)) atomicOr(&a.ctl->err, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stations and fault stations of the current level (io_recv_keep,
+// io_funcs.cu:428-469, including its use of corner 5 in place of corner 4;
+// io_fault_recv_keep, io_funcs.cu:2313-2351)
+__global__ void k_record(const StationArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rec = a.ctl->nrec;
+  const StationDev &S = a.st;
+  if (rec >= S.max_rec) return;
+  if (t < S.n * 9) {
+    const int n = t / 9, c = t % 9;
+    const long *ix = S.idx + (long)n * 8;
+    const float Lx2 = S.w[3 * n], Ly2 = S.w[3 * n + 1], Lz2 = S.w[3 * n + 2];
+    const float Lx1 = 1.0f - Lx2, Ly1 = 1.0f - Ly2, Lz1 = 1.0f - Lz2;
+    const float *v = a.w + (long)c * a.g.scmp;
+    const float b0 = v[ix[0]], b1 = v[ix[1]], b2 = v[ix[2]], b3 = v[ix[3]];
+    const float b5 = v[ix[5]], b6 = v[ix[6]], b7 = v[ix[7]];
+    const float r = b0 * Lx1 * Ly1 * Lz1 + b1 * Lx2 * Ly1 * Lz1 + b2 * Lx1 * Ly2 * Lz1 + b3 * Lx2 * Ly2 * Lz1 +
+                    b5 * Lx1 * Ly1 * Lz2 + b5 * Lx2 * Ly1 * Lz2 + b6 * Lx1 * Ly2 * Lz2 + b7 * Lx2 * Ly2 * Lz2;
+    S.seis[(long)t * S.max_rec + rec] = r;
+    if (!isfinite(r)) atomicOr(&a.ctl->err, 1);
+  } else if (t < S.n * 9 + S.nf * 9) {
+    const int u = t - S.n * 9, n = u / 9, c = u % 9;
+    const float *o = a.fout[S.fid[n]] + (long)c * a.ns;
+    const int *ix = S.fidx + 4 * n;
+    const float Ly2 = S.fw[2 * n], Lz2 = S.fw[2 * n + 1], Ly1 = 1.0f - Ly2, Lz1 = 1.0f - Lz2;
+    S.fseis[(long)u * S.max_rec + rec] = o[ix[0]] * Ly1 * Lz1 + o[ix[1]] * Ly2 * Lz1 + o[ix[2]] * Ly1 * Lz2 + o[ix[3]] * Ly2 * Lz2;
+  }
+}
+
+__global__ void k_advance(Ctl *c, int max_rec) {
+  c->it += 1;
+  if (c->nrec < max_rec) c->nrec += 1;
+}
+
+// ---------------------------------------------------------------------------
+void launch_fault_stage(const FaultArgs &a, cudaStream_t st) {
+  {
+    dim3 blk(32, 4), grd((a.g.nj + 31) / 32, (a.g.nk + 3) / 4);
+    k_fault_weld<<<grd, blk, 0, st>>>(a);
+  }
+  if (a.nj > 0 && a.nk > 0) {
+    dim3 blk(32, 4), grd((a.nj + 31) / 32, (a.nk + 3) / 4);
+    k_fault_vel<<<grd, blk, 0, st>>>(a);
+    k_fault_stress<<<grd, blk, 0, st>>>(a);
+  }
+}
+
+void launch_record(const StationArgs &a, cudaStream_t st) {
+  const int n = (a.st.n + a.st.nf) * 9;
+  if (n > 0 && a.st.max_rec > 0) k_record<<<(n + 127) / 128, 128, 0, st>>>(a);
+}
+
+void launch_advance(Ctl *c, int max_rec, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(c, max_rec); }
+
+}  // namespace cgfd

@@ -1,0 +1,103 @@
+// ops.cuh -- finite-difference operators of the MacCormack/DRP scheme
+// (src/forward/fd_t.h:9-140, tables in src/forward/fd_t.cu:64-110) as
+// sm_100a device functions, plus the argument blocks of the stage kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/cgfd.h"
+#include "common.h"
+
+namespace cgfd {
+
+// one-sided 5-point DRP derivative, forward (F = 1: offsets -1..3) or
+// backward (F = 0: offsets -3..1)
+constexpr float kC1 = -0.291647047f, kC2 = -0.666745142f, kC3 = 1.250117713f,
+                kC4 = -0.333411808f, kC5 = 0.041686285f;
+// 2-point and 3-point one-sided operators (MAC22, MAC24)
+constexpr float kB1 = -7.0f / 6.0f, kB2 = 8.0f / 6.0f, kB3 = -1.0f / 6.0f;
+// one-sided traction-image weights at split nodes
+constexpr float kA0 = 1.2500392377f, kA1 = 1.5417647610f, kA2 = -0.3334118088f,
+                kA3 = 0.0416862855f;
+
+template <int F>
+__device__ __forceinline__ float drp(const float *__restrict__ p, long s) {
+  if (F)
+    return kC1 * __ldg(p - s) + kC2 * __ldg(p) + kC3 * __ldg(p + s) + kC4 * __ldg(p + 2 * s) + kC5 * __ldg(p + 3 * s);
+  else
+    return -(kC1 * __ldg(p + s) + kC2 * __ldg(p) + kC3 * __ldg(p - s) + kC4 * __ldg(p - 2 * s) + kC5 * __ldg(p - 3 * s));
+}
+__device__ __forceinline__ float drp_rt(const float *p, long s, int f) {
+  return f ? drp<1>(p, s) : drp<0>(p, s);
+}
+__device__ __forceinline__ float mac22(const float *p, long s, int f) {
+  return f ? (__ldg(p + s) - __ldg(p)) : (__ldg(p) - __ldg(p - s));
+}
+__device__ __forceinline__ float mac24(const float *p, long s, int f) {
+  return f ? (kB1 * __ldg(p) + kB2 * __ldg(p + s) + kB3 * __ldg(p + 2 * s))
+           : -(kB1 * __ldg(p) + kB2 * __ldg(p - s) + kB3 * __ldg(p - 2 * s));
+}
+// DRP on register values v[-3..3] centred at v
+__device__ __forceinline__ float drp_v(const float *v, int f) {
+  return f ? (kC1 * v[-1] + kC2 * v[0] + kC3 * v[1] + kC4 * v[2] + kC5 * v[3])
+           : -(kC1 * v[1] + kC2 * v[0] + kC3 * v[-1] + kC4 * v[-2] + kC5 * v[-3]);
+}
+
+// offsets of the DRP stencil in table order and the matching weights
+__device__ __forceinline__ int drp_off(int f, int n) { return f ? n - 1 : n - 3; }
+__device__ __forceinline__ float drp_w(int f, int n) {
+  const float wf[5] = { kC1, kC2, kC3, kC4, kC5 };
+  return f ? wf[n] : -wf[4 - n];
+}
+
+__device__ __forceinline__ void mv3(const float *__restrict__ m, const float *v, float *o) {
+  o[0] = __ldg(m + 0) * v[0] + __ldg(m + 1) * v[1] + __ldg(m + 2) * v[2];
+  o[1] = __ldg(m + 3) * v[0] + __ldg(m + 4) * v[1] + __ldg(m + 5) * v[2];
+  o[2] = __ldg(m + 6) * v[0] + __ldg(m + 7) * v[1] + __ldg(m + 8) * v[2];
+}
+
+// level slots
+enum { LP = 0, LA = 1, LB = 2, LE = 3 };
+// RK mode of a stage: first (out tmp & end from P), middle, last
+enum { RK_FIRST = 0, RK_MID = 1, RK_LAST = 2 };
+
+struct VolArgs {
+  Grid g;
+  const float *cur, *pre;
+  float *out, *end;            // next-stage level (null at the last stage), E
+  const float *met, *med, *free_mat;
+  float ca, cb;
+  int isfree;
+  int nfault;
+  int fi0[MAXF];
+  const uint8_t *fflag[MAXF];
+  PmlFaceDev pml[6];           // indexed 2*dim + side; `on` = 0 when absent
+};
+
+struct FaultArgs {
+  Grid g;
+  FaultDev F;
+  const float *wcur, *wpre;
+  float *wout, *wend;
+  const float *met, *med, *free_mat;
+  // fault wavefield levels [9][2 sides][ny*nz]: stage input, time-n level,
+  // next-stage output (null at the last stage), end accumulator
+  const float *fc, *fp;
+  float *fo, *fe;
+  int idir, jdir, kdir;
+  int mode;
+  float ca, cb, rkb, dt;
+  int isfree, imethod;
+  int j0, k0, nj, nk;          // launch box of split nodes (interior indices)
+  Ctl *ctl;
+};
+
+struct StationArgs {
+  Grid g;
+  StationDev st;
+  const float *w;
+  const float *fout[MAXF];
+  long ns;
+  Ctl *ctl;
+};
+
+}  // namespace cgfd

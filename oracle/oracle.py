@@ -27,7 +27,7 @@ def load(double=False):
         return _libs[name]
     path = os.path.join(HERE, "_build", name)
     if not os.path.exists(path):
-        from build import build  # type: ignore
+        from build_oracle import build  # type: ignore
         build()
     lib = C.CDLL(path)
     vp = C.c_void_p

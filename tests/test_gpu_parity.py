@@ -1,0 +1,114 @@
+"""Parity of the CUDA path (libcgfd.so, through the C ABI) with the CPU
+oracle on the same seeded inputs.
+
+Tolerances: relative L2 <= 1e-4 for slip rate, slip, rupture time and
+station velocity (the bar of the forward path); <= 2e-5 for whole
+wavefields after a few steps from a random state.
+"""
+import numpy as np
+import pytest
+
+import inputs
+from cgfd import Solver, WAVE_COMPONENTS
+from oracle import OracleSolver
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-30))
+
+
+def _pair(prob):
+    return Solver(prob), OracleSolver(prob)
+
+
+@pytest.mark.parametrize("method,free", [(2, 1), (1, 1), (2, 0)])
+def test_random_state_steps(cgfd_lib, oracle_built, method, free):
+    """Eight steps (all eight operator pairs) from a random wavefield: every
+    volume, boundary and fault operator contributes."""
+    p = inputs.small_planar(nt=10, dynamic_method=method, free_surface=free)
+    rng = np.random.default_rng(11)
+    g, o = _pair(p)
+    for c in range(9):
+        scale = 1e-3 if c < 3 else 1e3
+        f = (rng.standard_normal((p.nk, p.nj, p.ni)) * scale).astype(np.float32)
+        g.set_wavefield(c, f)
+        o.set_wavefield(c, f)
+    for step in range(8):
+        g.run(1)
+        o.run(1)
+        for c in range(9):
+            e = rel_l2(g.wavefield(c), o.wavefield(c))
+            assert e < 2e-5, f"step {step} {WAVE_COMPONENTS[c]} rel-L2 {e:.2e}"
+
+
+@pytest.mark.parametrize("method,free", [(2, 1), (1, 1), (2, 0)])
+def test_rupture_small(cgfd_lib, oracle_built, method, free):
+    nt = 80
+    p = inputs.small_planar(nt=nt, dynamic_method=method, free_surface=free)
+    g, o = _pair(p)
+    vs_g, vs_o = [], []
+    for _ in range(nt // 10):
+        g.run(10)
+        o.run(10)
+        vs_g.append(g.fault("Vs"))
+        vs_o.append(o.fault("Vs"))
+    vs_g, vs_o = np.array(vs_g), np.array(vs_o)
+    assert vs_o.max() > 0.1, "no rupture in the oracle run"
+    assert rel_l2(vs_g, vs_o) < TOL
+    for f in ("Slip", "Slip1", "Peak_vs", "Tn", "Ts1"):
+        assert rel_l2(g.fault(f), o.fault(f)) < TOL, f
+    t0g, t0o = g.fault("Init_t0"), o.fault("Init_t0")
+    rup = t0o > 0
+    assert rup.sum() > 20
+    assert np.array_equal(t0g > 0, rup)
+    assert rel_l2(t0g[rup], t0o[rup]) < TOL
+    sg, so = g.stations(), o.stations()
+    assert sg.shape == so.shape == (len(p.stations), 9, nt)
+    assert rel_l2(sg[:, :3], so[:, :3]) < TOL
+    fg, fo = g.fault_stations(), o.fault_stations()
+    assert rel_l2(fg, fo) < TOL
+    for c in range(9):
+        assert rel_l2(g.wavefield(c), o.wavefield(c)) < TOL, WAVE_COMPONENTS[c]
+
+
+def test_checkpoint_restore(cgfd_lib):
+    p = inputs.small_planar(nt=40)
+    g = Solver(p)
+    g.run(13)
+    buf = g.checkpoint()
+    g.run(20)
+    ref = g.fault("Slip").copy(), g.wavefield("Vy").copy()
+    g.restore(buf)
+    assert g.steps_done == 13
+    g.run(20)
+    assert np.array_equal(g.fault("Slip"), ref[0])
+    assert np.array_equal(g.wavefield("Vy"), ref[1])
+
+
+def test_graph_and_direct_launch_agree(cgfd_lib, monkeypatch):
+    p = inputs.small_planar(nt=20)
+    g1 = Solver(p)
+    g1.run(17)
+    monkeypatch.setenv("CGFD_NO_GRAPH", "1")
+    g2 = Solver(p)
+    g2.run(17)
+    assert np.array_equal(g1.fault("Vs"), g2.fault("Vs"))
+    assert np.array_equal(g1.wavefield("Txy"), g2.wavefield("Txy"))
+
+
+def test_unstable_run_reports_error(cgfd_lib):
+    p = inputs.small_planar(nt=400, dt=0.05)
+    p.check_stability = 0
+    g = Solver(p)
+    with pytest.raises(Exception, match="ERR_UNSTABLE"):
+        g.run(400)
+
+
+def test_dt_above_limit_rejected(cgfd_lib):
+    p = inputs.small_planar(nt=10, dt=0.05)
+    with pytest.raises(Exception, match="ERR_DT"):
+        Solver(p)
