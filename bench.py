@@ -1,0 +1,262 @@
+"""Benchmark of the forward dynamic-rupture time step on B200.
+
+Workload (default): the 600x300x240 curvilinear case -- Gaussian-hill
+topography, four-layer medium with a 3% smoothed perturbation, vertical
+split-node fault of 400x180 nodes with linear slip-weakening friction,
+20-layer CFS-PML, traction-image free surface, 32 stations -- built from
+seeded synthetic inputs (gpu-cgfd3d-dynamic_b200/inputs.py: hills_layered).
+A step is one full time step (4 RK stages) of the whole domain.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  value = grid-point updates per second over
+the K timed steps (CUDA events on the solver's stream, max over ranks);
+inputs (6.6 GB of wavefield levels per GPU) exceed the 126 MB L2, so no
+flush is needed between steps.  --gpus N runs N independent replicas (one
+per GPU): the forward path does not shard.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gpu-cgfd3d-dynamic_b200")
+sys.path.insert(0, PKG)
+
+BYTES_PER_POINT_STEP = 768          # algorithmic HBM traffic of one point and step (FP32)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hills", choices=["hills", "tpv"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end run (default: --steps)")
+    return ap.parse_args()
+
+
+def make_problem(workload):
+    import inputs
+    if workload == "tpv":
+        return inputs.tpv_planar(), "tpv_planar 160x100x80 (x strike, y normal, z depth), h=200 m, homogeneous, planar fault"
+    return inputs.hills_layered(), ("hills_layered 600x300x240 (x strike, y normal, z depth), h=100 m, "
+                                    "8 Gaussian hills, 4-layer medium +3% perturbation, 400x180-node fault, "
+                                    "20-layer CFS-PML, free surface, 32 stations")
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, x):
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed
+    region."""
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 9]
+        os.unlink(self.f.name)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        load = [r for r in rows if r[4].strip().isdigit() and int(r[4]) >= 50] or rows
+        sm = [float(r[1]) for r in load if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = sorted({n for r in load for n, v in zip(names, r[6:10]) if v.strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(load)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(points):
+    """DRAM bytes of one volume-stage launch, from the committed ncu summary
+    (captured on a smaller case and scaled by grid points)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "volume_stage_traffic.json")) as f:
+            d = json.load(f)
+        return d["dram_bytes_per_launch"] * points / d["points"]
+    except Exception:
+        return None
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def oracle_rate(prob, steps, warmup, budget_s=150.0):
+    """CPU oracle on the same problem; returns (Gpt/s, cores, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import OracleSolver
+    th = cpu_threads()
+    o = OracleSolver(prob, threads=th)
+    for _ in range(min(warmup, 1)):
+        o.run(1)
+    t = time.perf_counter()
+    o.run(1)
+    one = time.perf_counter() - t
+    n = 1
+    more = max(0, min(steps, int(budget_s / max(one, 1e-3))) - 1)
+    if more:
+        t = time.perf_counter()
+        o.run(more)
+        one = (one + (time.perf_counter() - t)) / (1 + more)
+        n += more
+    o.close()
+    return prob.points / one / 1e9, th, f"{n} full time step(s) of the same problem after set-up, {th} OpenMP threads"
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    prob, desc = make_problem(args.workload)
+    metric, unit = "Gpt-updates/s", "Gpt/s"
+    config = {"workload": desc, "grid": [prob.nj, prob.ni, prob.nk], "points": prob.points,
+              "dt": prob.dt, "dynamic_method": prob.dynamic_method,
+              "l2": "inputs larger than L2 (6.6 GB of wavefield levels), no flush",
+              "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        v, th, sample = oracle_rate(prob, args.steps, args.warmup)
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": unit, "cores": th, "kind": "port", "sample": sample},
+                "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "the reference has no CPU implementation; the CPU oracle restating its "
+                        "algorithm stands in for it"}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import cgfd
+    torch.cuda.set_device(local)
+    setup = cgfd.Setup(prob)
+    s = cgfd.Solver(prob, setup=setup)
+    s.run(args.warmup)
+    s.set_timing(True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    s.run(args.steps)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(ws)
+    run_ms, vol_ms, vol_n = s.last_timing()
+    launches = s.last_launches()
+    run_ms_max = allmax(ws, run_ms)
+    vol_ms_max = allmax(ws, vol_ms)
+    value = prob.points * args.steps * ws / (run_ms_max / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    bytes_per_launch = prob.points * BYTES_PER_POINT_STEP / 4     # 4 stage launches per step
+    achieved = bytes_per_launch / (vol_ms_max / vol_n / 1e3) / 1e9
+    tr = traffic_per_launch(prob.points)
+    s.close()
+
+    # end to end through the C ABI with host buffers: upload of the prepared
+    # problem, then per step one cgfd_run and the read-back of the 11 fault
+    # fields (the reference's per-step fault output), stations at the end --
+    # the span of the reference's own timed region (drv_rk_curv_col_allstep)
+    ke = args.e2e_steps or args.steps
+    nbytes_f = 11 * prob.nk * prob.nj * 4
+    pinned = torch.empty(nbytes_f // 4, dtype=torch.float32, pin_memory=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = cgfd.Solver(prob, setup=setup)
+    for _ in range(ke):
+        s2.run(1)
+        s2.fault_all(out_ptr=pinned.data_ptr())
+    seis = s2.stations()
+    torch.cuda.synchronize()
+    e2e_s = allmax(ws, time.perf_counter() - t0)
+    s2.close()
+    up = setup.upload_bytes
+    e2e = {"value": prob.points * ke * ws / e2e_s / 1e9, "unit": unit,
+           "h2d_bytes_per_step": int(up / ke), "d2h_bytes_per_step": int(nbytes_f + seis.nbytes / ke),
+           "steps": ke, "note": "upload of the prepared problem amortised over the steps; host set-up excluded"}
+
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": run_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+            "roofline": {"bound": "hbm", "kernel": "k_volume (fused volume stage)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": tr, "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "volume_share_of_step": vol_ms_max / run_ms_max},
+            "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, th, sample = oracle_rate(prob, 1, 0, budget_s=30.0)
+        line["cpu_baseline"] = {"value": v, "unit": unit, "cores": th, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -213,6 +213,14 @@ def load_library(path: str = LIB_PATH):
     lib.cgfd_destroy.argtypes = [vp]
     lib.cgfd_destroy.restype = None
     lib.cgfd_last_error.restype = C.c_char_p
+    lib.cgfd_prepare.argtypes = [C.POINTER(CgfdConfig), C.POINTER(vp)]
+    lib.cgfd_setup_bytes.argtypes = [vp, C.POINTER(C.c_ulonglong)]
+    lib.cgfd_setup_dt_max.argtypes = [vp, _fp]
+    lib.cgfd_upload.argtypes = [vp, C.POINTER(vp)]
+    lib.cgfd_setup_free.argtypes = [vp]
+    lib.cgfd_setup_free.restype = None
+    lib.cgfd_set_timing.argtypes = [vp, C.c_int]
+    lib.cgfd_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     _lib = lib
     return lib
 
@@ -221,16 +229,64 @@ def _fptr(a):
     return a.ctypes.data_as(_fp)
 
 
-class Solver:
-    """A forward dynamic-rupture run on the current CUDA device."""
+class Setup:
+    """Host-side set-up of a problem (cgfd_prepare); needs no GPU."""
 
     def __init__(self, prob: Problem, lib=None):
         self.lib = lib or load_library()
         self.prob = prob
         self._cfg = prob.to_config()
         h = C.c_void_p()
-        self._check(self.lib.cgfd_create(C.byref(self._cfg), C.byref(h)))
+        rc = self.lib.cgfd_prepare(C.byref(self._cfg), C.byref(h))
+        if rc != 0:
+            raise CgfdError(f"{ERRORS.get(rc, rc)}: {self.lib.cgfd_last_error().decode()}")
         self.h = h
+
+    @property
+    def upload_bytes(self):
+        v = C.c_ulonglong()
+        self.lib.cgfd_setup_bytes(self.h, C.byref(v))
+        return v.value
+
+    def dt_max(self):
+        v = C.c_float()
+        self.lib.cgfd_setup_dt_max(self.h, C.byref(v))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cgfd_setup_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """A forward dynamic-rupture run on the current CUDA device."""
+
+    def __init__(self, prob: Problem, lib=None, setup: Setup = None):
+        self.lib = lib or load_library()
+        self.prob = prob
+        h = C.c_void_p()
+        if setup is not None:
+            self._check(self.lib.cgfd_upload(setup.h, C.byref(h)))
+        else:
+            self._cfg = prob.to_config()
+            self._check(self.lib.cgfd_create(C.byref(self._cfg), C.byref(h)))
+        self.h = h
+
+    def set_timing(self, on=True):
+        self._check(self.lib.cgfd_set_timing(self.h, int(bool(on))))
+
+    def last_timing(self):
+        """(run_ms, volume_ms, volume_launches) of the last run()."""
+        a, b, n = C.c_double(), C.c_double(), C.c_longlong()
+        self._check(self.lib.cgfd_last_timing(self.h, C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value
 
     def _check(self, rc):
         if rc != 0:
@@ -259,8 +315,13 @@ class Solver:
         self._check(self.lib.cgfd_get_fault(self.h, fault_id, field, _fptr(out)))
         return out
 
-    def fault_all(self, fault_id=0, out=None):
+    def fault_all(self, fault_id=0, out=None, out_ptr=None):
+        """All 11 fault fields [11, nk, nj]; ``out_ptr`` (an address) lets the
+        caller pass pinned host memory."""
         p = self.prob
+        if out_ptr is not None:
+            self._check(self.lib.cgfd_get_fault_all(self.h, fault_id, C.cast(out_ptr, _fp)))
+            return None
         if out is None:
             out = np.empty((11, p.nk, p.nj), np.float32)
         self._check(self.lib.cgfd_get_fault_all(self.h, fault_id, _fptr(out)))

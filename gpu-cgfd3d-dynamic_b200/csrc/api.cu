@@ -20,7 +20,9 @@
 #include "setup.h"
 
 namespace cgfd {
-void launch_volume(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume(const VolArgs &interior, const VolArgs &shell, int idir, int jdir, int kdir, int mode,
+                   cudaStream_t st);
+void volume_boxes(VolArgs &a, const int (*boxes)[6], int n);
 void launch_fault_stage(const FaultArgs &a, cudaStream_t st);
 void launch_record(const StationArgs &a, cudaStream_t st);
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
@@ -69,11 +71,22 @@ struct cgfd_solver {
   float *seis = nullptr, *fseis = nullptr;
   Ctl *ctl = nullptr;
   cudaStream_t stream = nullptr;
-  cudaGraphExec_t graph[8] = {};
+  cudaGraphExec_t graph[2][8] = {};     // [timing][it % 8]
   bool use_graph = true;
+  int timing = 0;
+  cudaEvent_t ev_run[2] = {};
+  cudaEvent_t ev_vol[8][4][2] = {};
+  double run_ms = 0, vol_ms = 0;
+  long long vol_launches = 0;
   int it = 0;
   long long launches_per_step = 0, last_launches = 0;
+  int box_in[1][6];                     // interior box (no PML, no surface rows)
+  int box_shell[6][6];                  // PML slabs and surface rows
   std::vector<void *> allocs;
+};
+
+struct cgfd_setup {
+  cgfd::HostSetup H;
 };
 
 namespace {
@@ -94,7 +107,10 @@ int slot(int L, int it) {
 
 void destroy(cgfd_solver *s) {
   if (!s) return;
-  for (int q = 0; q < 8; q++) if (s->graph[q]) cudaGraphExecDestroy(s->graph[q]);
+  for (int t = 0; t < 2; t++) for (int q = 0; q < 8; q++) if (s->graph[t][q]) cudaGraphExecDestroy(s->graph[t][q]);
+  for (int q = 0; q < 2; q++) if (s->ev_run[q]) cudaEventDestroy(s->ev_run[q]);
+  for (int a = 0; a < 8; a++) for (int b = 0; b < 4; b++) for (int c = 0; c < 2; c++)
+    if (s->ev_vol[a][b][c]) cudaEventDestroy(s->ev_vol[a][b][c]);
   for (void *p : s->allocs) cudaFree(p);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -141,8 +157,15 @@ void enqueue_step(cgfd_solver *s, int it) {
       v.pml[q].acur = s->pml[q].aux[scur]; v.pml[q].apre = s->pml[q].aux[spre];
       v.pml[q].aout = sout >= 0 ? s->pml[q].aux[sout] : nullptr; v.pml[q].aend = s->pml[q].aux[send];
     }
-    launch_volume(v, idir, jdir, kdir, mode, s->stream);
-    nl++;
+    // external event nodes when captured, so that the events really fire
+    // on every graph replay
+    VolArgs vi = v, vs = v;
+    volume_boxes(vi, s->box_in, 1);
+    volume_boxes(vs, s->box_shell, 6);
+    if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
+    launch_volume(vi, vs, idir, jdir, kdir, mode, s->stream);
+    if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
+    nl += (vi.nbox > 0) + (vs.nbox > 0);
   }
   launch_advance(s->ctl, s->st.max_rec, s->stream);
   nl++;
@@ -174,6 +197,36 @@ void cgfd_config_default(cgfd_config *c) {
 
 const char *cgfd_last_error(void) { return g_err.c_str(); }
 
+int cgfd_prepare(const cgfd_config *cfg, cgfd_setup **out) {
+  if (!cfg || !out) return fail(CGFD_ERR_ARG, "null argument");
+  *out = nullptr;
+  cgfd_setup *su = new cgfd_setup();
+  std::string msg;
+  int rc = build_setup(cfg, su->H, msg);
+  if (rc != CGFD_OK) { delete su; return fail(rc, msg); }
+  *out = su;
+  return CGFD_OK;
+}
+
+void cgfd_setup_free(cgfd_setup *su) { delete su; }
+
+int cgfd_setup_dt_max(const cgfd_setup *su, float *d) {
+  if (!su || !d) return fail(CGFD_ERR_ARG, "bad argument");
+  *d = su->H.dtmax;
+  return CGFD_OK;
+}
+
+int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes) {
+  if (!su || !bytes) return fail(CGFD_ERR_ARG, "bad argument");
+  const HostSetup &H = su->H;
+  unsigned long long n = (H.metric.size() + H.media.size() + H.free_mat.size()) * 4ull;
+  for (int d = 0; d < 3; d++) for (int q = 0; q < 2; q++) n += 3ull * (H.pml[d][q].A.size()) * 4;
+  for (auto &F : H.faults) n += F.flag.size() + (F.mat.size() + F.fmat.size() + F.scal.size() + F.out.size()) * 4ull;
+  n += H.sta_idx.size() * sizeof(long) + (H.sta_w.size() + H.fsta_w.size()) * 4ull + (H.fsta_fid.size() + H.fsta_idx.size()) * 4ull;
+  *bytes = n;
+  return CGFD_OK;
+}
+
 int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
   if (!cfg || !out) return fail(CGFD_ERR_ARG, "null argument");
   *out = nullptr;
@@ -182,11 +235,23 @@ int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
     cudaGetLastError();
     return fail(CGFD_ERR_NODEVICE, "no CUDA device visible");
   }
-  HostSetup H;
-  std::string msg;
-  int rc = build_setup(cfg, H, msg);
-  if (rc != CGFD_OK) return fail(rc, msg);
+  cgfd_setup *su = nullptr;
+  int rc = cgfd_prepare(cfg, &su);
+  if (rc != CGFD_OK) return rc;
+  rc = cgfd_upload(su, out);
+  cgfd_setup_free(su);
+  return rc;
+}
 
+int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
+  if (!su || !out) return fail(CGFD_ERR_ARG, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CGFD_ERR_NODEVICE, "no CUDA device visible");
+  }
+  const HostSetup &H = su->H;
   cgfd_solver *s = new cgfd_solver();
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { destroy(s); return cuda_fail(e, "stream"); }
@@ -266,7 +331,26 @@ int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
   }
   st.idx = s->sta_idx; st.w = s->sta_w; st.fid = s->fsta_fid; st.fidx = s->fsta_idx; st.fw = s->fsta_w;
   st.seis = s->seis; st.fseis = s->fseis;
+  // interior box and shell boxes (interior indices, inclusive)
+  {
+    auto L = [&](int d, int sd) { return H.pml[d][sd].on ? H.pml[d][sd].L + 1 : 0; };
+    const int ilo = L(0, 0), ihi = g.ni - 1 - L(0, 1), jlo = L(1, 0), jhi = g.nj - 1 - L(1, 1);
+    const int klo = L(2, 0), khi = s->isfree ? g.nk - 5 : g.nk - 1 - L(2, 1);
+    const int bi[6] = { ilo, ihi, jlo, jhi, klo, khi };
+    std::memcpy(s->box_in[0], bi, sizeof bi);
+    const int sh[6][6] = {
+      { 0, ilo - 1, 0, g.nj - 1, 0, g.nk - 1 },
+      { ihi + 1, g.ni - 1, 0, g.nj - 1, 0, g.nk - 1 },
+      { ilo, ihi, 0, jlo - 1, 0, g.nk - 1 },
+      { ilo, ihi, jhi + 1, g.nj - 1, 0, g.nk - 1 },
+      { ilo, ihi, jlo, jhi, 0, klo - 1 },
+      { ilo, ihi, jlo, jhi, khi + 1, g.nk - 1 } };
+    std::memcpy(s->box_shell, sh, sizeof sh);
+  }
   CK(dalloc(s, &s->ctl, 1), "control block");
+  for (int q = 0; q < 2; q++) CK(cudaEventCreate(&s->ev_run[q]), "event");
+  for (int a = 0; a < 8; a++) for (int b = 0; b < 4; b++) for (int c = 0; c < 2; c++)
+    CK(cudaEventCreate(&s->ev_vol[a][b][c]), "event");
   CK(cudaStreamSynchronize(s->stream), "set-up");
 #undef CK
   *out = s;
@@ -276,13 +360,17 @@ int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
 int cgfd_run(cgfd_solver *s, int nsteps) {
   if (!s || nsteps < 0) return fail(CGFD_ERR_ARG, "bad argument");
   long long nl = 0;
+  double vol_ms = 0;
+  long long vol_n = 0;
+  cudaError_t e = cudaEventRecord(s->ev_run[0], s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "event");
   for (int q = 0; q < nsteps; q++) {
     const int it = s->it;
     if (s->use_graph) {
-      cudaGraphExec_t &G = s->graph[it % 8];
+      cudaGraphExec_t &G = s->graph[s->timing][it % 8];
       if (!G) {
         cudaGraph_t gr;
-        cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+        e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_fail(e, "begin capture");
         enqueue_step(s, it);
         e = cudaStreamEndCapture(s->stream, &gr);
@@ -291,24 +379,55 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
         cudaGraphDestroy(gr);
         if (e != cudaSuccess) { G = nullptr; return cuda_fail(e, "instantiate"); }
       }
-      cudaError_t e = cudaGraphLaunch(G, s->stream);
+      e = cudaGraphLaunch(G, s->stream);
       if (e != cudaSuccess) return cuda_fail(e, "graph launch");
     } else {
       enqueue_step(s, it);
-      cudaError_t e = cudaGetLastError();
+      e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "launch");
+    }
+    if (s->timing) {
+      // the events of this step are reused by the next step of the same
+      // operator pair, so read them now
+      e = cudaEventSynchronize(s->ev_vol[it % 8][3][1]);
+      if (e != cudaSuccess) return cuda_fail(e, "timing");
+      for (int st = 0; st < 4; st++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, s->ev_vol[it % 8][st][0], s->ev_vol[it % 8][st][1]);
+        vol_ms += ms;
+        vol_n++;
+      }
     }
     nl += s->launches_per_step;
     s->it++;
   }
+  e = cudaEventRecord(s->ev_run[1], s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "event");
   s->last_launches = nl;
-  cudaError_t e = cudaStreamSynchronize(s->stream);
+  e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "run");
+  float run_ms = 0;
+  cudaEventElapsedTime(&run_ms, s->ev_run[0], s->ev_run[1]);
+  s->run_ms = run_ms; s->vol_ms = vol_ms; s->vol_launches = vol_n;
   Ctl c;
   e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read control block");
   if (c.it != s->it) return fail(CGFD_ERR_STATE, "device step counter out of step with the host");
   if (c.err & 1) return fail(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
+  return CGFD_OK;
+}
+
+int cgfd_set_timing(cgfd_solver *s, int on) {
+  if (!s) return fail(CGFD_ERR_ARG, "bad argument");
+  s->timing = on ? 1 : 0;
+  return CGFD_OK;
+}
+
+int cgfd_last_timing(const cgfd_solver *s, double *run_ms, double *volume_ms, long long *volume_launches) {
+  if (!s) return fail(CGFD_ERR_ARG, "bad argument");
+  if (run_ms) *run_ms = s->run_ms;
+  if (volume_ms) *volume_ms = s->vol_ms;
+  if (volume_launches) *volume_launches = s->vol_launches;
   return CGFD_OK;
 }
 
@@ -328,13 +447,14 @@ int cgfd_get_fault_all(cgfd_solver *s, int f, float *out) {
   if (!s || !out || f < 0 || f >= (int)s->faults.size()) return fail(CGFD_ERR_ARG, "bad argument");
   const Grid &g = s->g;
   const size_t ns = (size_t)g.ny * g.nz;
-  std::vector<float> h((size_t)CGFD_FAULT_NFIELD * ns);
-  cudaError_t e = cudaMemcpyAsync(h.data(), s->faults[f].out, h.size() * 4, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  for (int q = 0; q < CGFD_FAULT_NFIELD; q++) {
+    const float *src = s->faults[f].out + q * ns + (size_t)NG * g.ny + NG;
+    cudaError_t e = cudaMemcpy2DAsync(out + (size_t)q * g.nk * g.nj, (size_t)g.nj * 4, src, (size_t)g.ny * 4,
+                                      (size_t)g.nj * 4, g.nk, cudaMemcpyDeviceToHost, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "read fault");
+  }
+  cudaError_t e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read fault");
-  for (int q = 0; q < CGFD_FAULT_NFIELD; q++)
-    for (int k = 0; k < g.nk; k++)
-      std::memcpy(out + ((size_t)q * g.nk + k) * g.nj, h.data() + q * ns + (size_t)(k + NG) * g.ny + NG, (size_t)g.nj * 4);
   return CGFD_OK;
 }
 

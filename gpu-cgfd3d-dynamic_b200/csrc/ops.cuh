@@ -60,8 +60,17 @@ enum { LP = 0, LA = 1, LB = 2, LE = 3 };
 // RK mode of a stage: first (out tmp & end from P), middle, last
 enum { RK_FIRST = 0, RK_MID = 1, RK_LAST = 2 };
 
+// a box of interior points (inclusive bounds) covered by one launch;
+// blocks [first, next box's first) belong to it
+struct VolBox {
+  int i0, i1, j0, j1, k0;
+  int nbx, nby, first;
+};
+
 struct VolArgs {
   Grid g;
+  int nbox, nblocks;
+  VolBox box[7];
   const float *cur, *pre;
   float *out, *end;            // next-stage level (null at the last stage), E
   const float *met, *med, *free_mat;

@@ -133,9 +133,23 @@ typedef struct cgfd_config {
 } cgfd_config;
 
 typedef struct cgfd_solver cgfd_solver;
+typedef struct cgfd_setup cgfd_setup;
 
 /* ABI version compiled into the library (CGFD_ABI_VERSION). */
 int cgfd_abi_version(void);
+
+/* Host half of cgfd_create: grid, metric, medium, PML, free-surface and
+ * fault set-up into host memory (main_curv_col_el_3d.cu:113-705).  Needs
+ * no GPU. */
+int cgfd_prepare(const cgfd_config *cfg, cgfd_setup **out);
+/* Bytes that cgfd_upload copies to the device. */
+int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes);
+/* Largest stable dt of a prepared problem (CFL 1.3). */
+int cgfd_setup_dt_max(const cgfd_setup *su, float *dtmax);
+/* Device half of cgfd_create: allocate the device state on the current
+ * device and copy the prepared problem (drv_rk_curv_col.cu:90-100). */
+int cgfd_upload(const cgfd_setup *su, cgfd_solver **out);
+void cgfd_setup_free(cgfd_setup *su);
 
 /* Fill cfg with the reference's defaults (welded margin 40, dynamic
  * method 2, stability check on, no PML, free surface off). */
@@ -195,6 +209,15 @@ int cgfd_restore(cgfd_solver *s, const void *buf, unsigned long long bytes);
 
 /* Kernel launches issued by the last cgfd_run call (for accounting). */
 int cgfd_last_launches(const cgfd_solver *s, long long *launches);
+
+/* 1: time every volume-stage launch with CUDA events on the solver's
+ * stream (cgfd_run then waits for each step); 0: off (default). */
+int cgfd_set_timing(cgfd_solver *s, int on);
+/* Device time of the last cgfd_run (events on the solver's stream at its
+ * start and end) and, with timing on, the summed duration and count of its
+ * volume-stage launches. */
+int cgfd_last_timing(const cgfd_solver *s, double *run_ms, double *volume_ms,
+                     long long *volume_launches);
 
 /* Release device and host memory of the handle. */
 void cgfd_destroy(cgfd_solver *s);

@@ -335,6 +335,7 @@ real dist_point2plane(const real *x0, const real *x1, const real *x2, const real
 }
 void calc_dtmax(oracle_solver *S) {
   real best = (real)1.0e10;
+#pragma omp parallel for collapse(2) reduction(min:best)
   for (int k = S->nk1; k <= S->nk2; k++) for (int j = S->nj1; j <= S->nj2; j++)
     for (int i = S->ni1; i <= S->ni2; i++) {
       size_t p = S->I(i,j,k);
