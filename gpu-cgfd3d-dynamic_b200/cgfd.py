@@ -19,7 +19,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libcgfd.so")
+LIB_PATH = os.environ.get("CGFD_LIB", os.path.join(HERE, "lib", "libcgfd.so"))
 
 MAX_FAULTS = 8
 GRID_FAULT_PLANE = 0

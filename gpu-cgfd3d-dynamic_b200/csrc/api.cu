@@ -7,6 +7,7 @@
 // sample, 4 x (fault-plane kernels + fused volume kernel) and the step
 // counter advance.  Time levels P and E swap by step parity, which it % 8
 // fixes, so the graphs never need their arguments updated.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +24,11 @@ namespace cgfd {
 void launch_volume(const VolArgs &interior, const VolArgs &shell, int idir, int jdir, int kdir, int mode,
                    cudaStream_t st);
 void volume_boxes(VolArgs &a, const int (*boxes)[6], int n);
+void launch_volume_tiled(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void volume_tma_prepare();
+int volume_tma_encode(CUtensorMap *tm, const float *level, const Grid &g);
+void launch_volume_tma(const CUtensorMap &tm, const VolArgs &a, int idir, int jdir, int kdir, int mode,
+                       cudaStream_t st);
 void launch_fault_stage(const FaultArgs &a, cudaStream_t st);
 void launch_record(const StationArgs &a, cudaStream_t st);
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
@@ -80,6 +86,10 @@ struct cgfd_solver {
   long long vol_launches = 0;
   int it = 0;
   long long launches_per_step = 0, last_launches = 0;
+  int tiled = 2, kchunk = 32;           // volume kernel: 2 TMA-fed, 1 smem-tiled, 0 boxes
+  int kchunk_tma = 32;
+  int box_top[1][6];                    // rows under the free surface
+  CUtensorMap tmap[4];                  // TMA maps of the 4 level slots
   int box_in[1][6];                     // interior box (no PML, no surface rows)
   int box_shell[6][6];                  // PML slabs and surface rows
   std::vector<void *> allocs;
@@ -159,13 +169,31 @@ void enqueue_step(cgfd_solver *s, int it) {
     }
     // external event nodes when captured, so that the events really fire
     // on every graph replay
-    VolArgs vi = v, vs = v;
-    volume_boxes(vi, s->box_in, 1);
-    volume_boxes(vs, s->box_shell, 6);
     if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
-    launch_volume(vi, vs, idir, jdir, kdir, mode, s->stream);
+    VolArgs vi = v, vs = v;
+    v.kchunk = s->kchunk;
+    v.ctl_err = &s->ctl->err;
+    if (s->tiled == 2) {
+      // rows under the free surface go to the box kernel (traction image,
+      // velocity-low operators), everything below to the TMA kernel
+      v.kend = s->isfree ? s->g.nk - 4 : s->g.nk;
+      v.kchunk = s->kchunk_tma;
+      launch_volume_tma(s->tmap[scur], v, idir, jdir, kdir, mode, s->stream);
+      vi.nbox = 0;
+      volume_boxes(vs, s->box_top, 1);
+      VolArgs none = vs;
+      none.nbox = 0;
+      launch_volume(none, vs, idir, jdir, kdir, mode, s->stream);
+    } else if (s->tiled == 1) {
+      launch_volume_tiled(v, idir, jdir, kdir, mode, s->stream);
+      vi.nbox = 1; vs.nbox = 0;
+    } else {
+      volume_boxes(vi, s->box_in, 1);
+      volume_boxes(vs, s->box_shell, 6);
+      launch_volume(vi, vs, idir, jdir, kdir, mode, s->stream);
+    }
     if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
-    nl += (vi.nbox > 0) + (vs.nbox > 0);
+    nl += (vi.nbox > 0) + (vs.nbox > 0) + (s->tiled ? 1 : 0);
   }
   launch_advance(s->ctl, s->st.max_rec, s->stream);
   nl++;
@@ -258,10 +286,27 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   s->g = H.g; s->imethod = H.imethod; s->isfree = H.isfree; s->dt = H.dt; s->dtmax = H.dtmax;
   const char *ng = std::getenv("CGFD_NO_GRAPH");
   s->use_graph = !(ng && ng[0] == '1');
+  const char *vk = std::getenv("CGFD_VOLUME");
+  s->tiled = 0;
+  if (vk && std::strcmp(vk, "tma") == 0) s->tiled = 2;
+  if (vk && std::strcmp(vk, "tiled") == 0) s->tiled = 1;
+  {
+    // z chunk per block: enough blocks for several waves, rows >= 8
+    const long bxy = (long)((H.g.ni + 31) / 32) * ((H.g.nj + 7) / 8);
+    const long nch = std::max<long>(1, (2400 + bxy - 1) / bxy);
+    s->kchunk = (int)std::min<long>(64, std::max<long>(8, (H.g.nk + nch - 1) / nch));
+    const int nkt = H.isfree ? H.g.nk - 4 : H.g.nk;
+    s->kchunk_tma = (int)std::min<long>(64, std::max<long>(10, (nkt + nch - 1) / nch));
+  }
   const Grid &g = s->g;
   const size_t lev = (size_t)NCMP * g.scmp, ns = (size_t)g.ny * g.nz;
 #define CK(x, what) do { cudaError_t _e = (x); if (_e != cudaSuccess) { destroy(s); return cuda_fail(_e, what); } } while (0)
   for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
+  if (s->tiled == 2) {
+    volume_tma_prepare();
+    for (int L = 0; L < 4; L++)
+      if (volume_tma_encode(&s->tmap[L], s->w[L], g) != 0) { destroy(s); return fail(CGFD_ERR_CUDA, "tensor map encoding failed"); }
+  }
   CK(dalloc(s, &s->met, H.metric.size()), "metric");
   CK(dalloc(s, &s->med, H.media.size()), "medium");
   CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
@@ -346,6 +391,8 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
       { ilo, ihi, jlo, jhi, 0, klo - 1 },
       { ilo, ihi, jlo, jhi, khi + 1, g.nk - 1 } };
     std::memcpy(s->box_shell, sh, sizeof sh);
+    const int bt[6] = { 0, g.ni - 1, 0, g.nj - 1, s->isfree ? g.nk - 4 : g.nk, g.nk - 1 };
+    std::memcpy(s->box_top[0], bt, sizeof bt);
   }
   CK(dalloc(s, &s->ctl, 1), "control block");
   for (int q = 0; q < 2; q++) CK(cudaEventCreate(&s->ev_run[q]), "event");
@@ -413,7 +460,8 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read control block");
   if (c.it != s->it) return fail(CGFD_ERR_STATE, "device step counter out of step with the host");
-  if (c.err & 1) return fail(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
+  if (c.err & CTL_ERR_TMA) return fail(CGFD_ERR_CUDA, "volume kernel: a TMA row load did not complete in time");
+  if (c.err & CTL_ERR_NONFINITE) return fail(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
   return CGFD_OK;
 }
 

@@ -111,8 +111,9 @@ struct StationDev {
 struct Ctl {
   int it;                   // steps taken
   int nrec;                 // records taken
-  int err;                  // bit 0: non-finite value seen
+  int err;                  // CTL_ERR_* bits
   int pad;
 };
+enum CtlErr { CTL_ERR_NONFINITE = 1, CTL_ERR_TMA = 2 };
 
 }  // namespace cgfd

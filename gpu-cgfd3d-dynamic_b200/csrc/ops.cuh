@@ -69,6 +69,9 @@ struct VolBox {
 
 struct VolArgs {
   Grid g;
+  int kchunk;                  // z rows marched by one block (tiled kernels)
+  int kend;                    // rows [0, kend) handled by the TMA kernel
+  int *ctl_err;                // Ctl::err of the solver
   int nbox, nblocks;
   VolBox box[7];
   const float *cur, *pre;

@@ -17,8 +17,14 @@
 // domain is cut into boxes: the interior box (no PML, no surface rows) runs
 // k_volume<INTERIOR>, whose code holds no boundary logic, and the shell of
 // PML slabs and the top four rows runs k_volume<SHELL>.  Each stage reads
-// the input level (stencil halos come from L1/L2), the metric and the medium
+// the input level (stencil taps come from L1/L2), the metric and the medium
 // once and writes the output levels once.
+//
+// Each component's taps are addressed from one base pointer: x taps are
+// immediate offsets, y / z taps share two int offset tables, the centre
+// sample is loaded once for all three directions.  The RHS is built
+// direction by direction, so a PML face of normal d reuses direction d's
+// contribution.
 //
 // Roofline: HBM-bound.  Algorithmic traffic per point and step is
 // 192 floats = 768 B (21+18, 39+18, 39+18, 30+9 floats over the 4 stages).
@@ -45,51 +51,131 @@ __device__ __forceinline__ float ctrac(const float *__restrict__ w, const float 
                                        __ldg(met + (ax + 2) * sc + q) * __ldg(w + c2 * sc + q));
 }
 
-// Accumulate one direction's derivatives straight into the velocity
-// gradient G[c][b] = dV_c/dx_b and the momentum sums
-// s_r = sum_a e_a . d(sigma_row r)/dxi_a, so that only 12 accumulators stay
-// live instead of 27 derivatives.
 template <int F>
-__device__ __forceinline__ void acc_vel(const float *__restrict__ w, long sc, long st, const float ea[3],
-                                        float G[3][3], float dv[3]) {
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    const float d = drp<F>(w + (VX + c) * sc, st);
-    dv[c] = d;
-    G[c][0] += ea[0] * d; G[c][1] += ea[1] * d; G[c][2] += ea[2] * d;
-  }
-}
-template <int F>
-__device__ __forceinline__ void acc_stress(const float *__restrict__ w, long sc, long st, const float ea[3],
-                                           float s[3]) {
-  float d;
-  d = drp<F>(w + TXX * sc, st); s[0] += ea[0] * d;
-  d = drp<F>(w + TYY * sc, st); s[1] += ea[1] * d;
-  d = drp<F>(w + TZZ * sc, st); s[2] += ea[2] * d;
-  d = drp<F>(w + TYZ * sc, st); s[1] += ea[2] * d; s[2] += ea[1] * d;
-  d = drp<F>(w + TXZ * sc, st); s[0] += ea[2] * d; s[2] += ea[0] * d;
-  d = drp<F>(w + TXY * sc, st); s[0] += ea[1] * d; s[1] += ea[0] * d;
+__device__ __forceinline__ float wdrp(int n) {
+  return F ? (n == 0 ? kC1 : n == 1 ? kC2 : n == 2 ? kC3 : n == 3 ? kC4 : kC5)
+           : (n == 0 ? -kC5 : n == 1 ? -kC4 : n == 2 ? -kC3 : n == 3 ? -kC2 : -kC1);
 }
 
-__device__ __forceinline__ void hooke(const float G[3][3], float lam, float mu, float l2m, float h[9]) {
-  h[TXX] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]);
-  h[TYY] = l2m * G[1][1] + lam * (G[0][0] + G[2][2]);
-  h[TZZ] = l2m * G[2][2] + lam * (G[0][0] + G[1][1]);
-  h[TXY] = mu * (G[0][1] + G[1][0]);
-  h[TXZ] = mu * (G[0][2] + G[2][0]);
-  h[TYZ] = mu * (G[1][2] + G[2][1]);
+// one-sided DRP derivative of the component at wc with the centre sample v0
+// known; off[n] are the offsets of the 4 other taps in table order
+template <int F>
+__device__ __forceinline__ float drp_c(const float *__restrict__ wc, float v0, const int off[4]) {
+  // table order: F: -1, 0, 1, 2, 3; B: -3, -2, -1, 0, 1 (centre at n = 1 / 3)
+  if (F)
+    return kC1 * __ldg(wc + off[0]) + kC2 * v0 + kC3 * __ldg(wc + off[1]) + kC4 * __ldg(wc + off[2]) +
+           kC5 * __ldg(wc + off[3]);
+  else
+    return -(kC5 * __ldg(wc + off[0]) + kC4 * __ldg(wc + off[1]) + kC3 * __ldg(wc + off[2]) + kC2 * v0 +
+             kC1 * __ldg(wc + off[3]));
+}
+template <int F>
+__device__ __forceinline__ void tap_offsets(int s, int off[4]) {
+  if (F) { off[0] = -s; off[1] = s; off[2] = 2 * s; off[3] = 3 * s; }
+  else { off[0] = -3 * s; off[1] = -2 * s; off[2] = -s; off[3] = s; }
+}
+
+// direction-d part of the RHS from the nine d-derivatives D[c] and e = e_d
+__device__ __forceinline__ void rhs_dir(const float D[9], const float e[3], float lam, float mu, float l2m,
+                                        float slw, float r[9]) {
+  r[VX] = slw * (e[0] * D[TXX] + e[1] * D[TXY] + e[2] * D[TXZ]);
+  r[VY] = slw * (e[0] * D[TXY] + e[1] * D[TYY] + e[2] * D[TYZ]);
+  r[VZ] = slw * (e[0] * D[TXZ] + e[1] * D[TYZ] + e[2] * D[TZZ]);
+  r[TXX] = l2m * e[0] * D[VX] + lam * (e[1] * D[VY] + e[2] * D[VZ]);
+  r[TYY] = l2m * e[1] * D[VY] + lam * (e[0] * D[VX] + e[2] * D[VZ]);
+  r[TZZ] = l2m * e[2] * D[VZ] + lam * (e[0] * D[VX] + e[1] * D[VY]);
+  r[TXY] = mu * (e[1] * D[VX] + e[0] * D[VY]);
+  r[TXZ] = mu * (e[2] * D[VX] + e[0] * D[VZ]);
+  r[TYZ] = mu * (e[2] * D[VY] + e[1] * D[VZ]);
+}
+
+// Accumulate one direction's derivatives straight into the velocity
+// gradient G[c][b] = dV_c/dx_b and the momentum sums
+// s_r = sum_a e_a . d(sigma_row r)/dxi_a (12 live accumulators).
+template <int F>
+__device__ __forceinline__ void acc_dir(const float *__restrict__ w, long sc, const float v0[9], const int off[4],
+                                        const float ea[3], float G[3][3], float s[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float d = drp_c<F>(w + (VX + c) * sc, v0[VX + c], off);
+    G[c][0] += ea[0] * d; G[c][1] += ea[1] * d; G[c][2] += ea[2] * d;
+  }
+  float d;
+  d = drp_c<F>(w + TXX * sc, v0[TXX], off); s[0] += ea[0] * d;
+  d = drp_c<F>(w + TYY * sc, v0[TYY], off); s[1] += ea[1] * d;
+  d = drp_c<F>(w + TZZ * sc, v0[TZZ], off); s[2] += ea[2] * d;
+  d = drp_c<F>(w + TYZ * sc, v0[TYZ], off); s[1] += ea[2] * d; s[2] += ea[1] * d;
+  d = drp_c<F>(w + TXZ * sc, v0[TXZ], off); s[0] += ea[2] * d; s[2] += ea[0] * d;
+  d = drp_c<F>(w + TXY * sc, v0[TXY], off); s[0] += ea[1] * d; s[1] += ea[0] * d;
+}
+
+template <int F>
+__device__ __forceinline__ void derivs(const float *__restrict__ w, long sc, const float v0[9], const int off[4],
+                                       float D[9]) {
+#pragma unroll
+  for (int c = 0; c < 9; c++) D[c] = drp_c<F>(w + c * sc, v0[c], off);
+}
+
+// PML face P (normal d) at this point: add its correction to corr and
+// advance its auxiliary fields
+template <int MODE>
+__device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, int d, int I, int J, int K,
+                                         const float r[9], const float D[9], const float e2[3], float lam,
+                                         float mu, float l2m, bool surf, long fidx, float corr[9]) {
+  const int li = I - P.i1, lj = J - P.j1, lk = K - P.k1;
+  if (li < 0 || li >= P.fni || lj < 0 || lj >= P.fnj || lk < 0 || lk >= P.fnk) return;
+  const int layer = d == 0 ? li : (d == 1 ? lj : lk);
+  const float cA = __ldg(P.A + layer), cB = __ldg(P.B + layer), cD = __ldg(P.D + layer);
+  const long pa = li + (long)lj * P.fni + (long)lk * P.fni * P.fnj;
+  float ar[9];
+#pragma unroll
+  for (int c = 0; c < 9; c++) {
+    const float av = __ldg(P.acur + c * P.siz + pa);
+    corr[c] += (cB - 1.0f) * r[c] - cB * av;
+    ar[c] = cD * r[c] - cA * av;
+  }
+  if (surf) {
+    // free-surface coupling of the x / y faces: the d-derivative of the
+    // surface-converted dz velocity gradient
+    const float *X = a.free_mat + (long)(d == 0 ? 0 : 1) * a.g.ny * a.g.nx * 9 + fidx;
+    const float dd[3] = { D[VX], D[VY], D[VZ] };
+    float z[3];
+    mv3(X, dd, z);
+    float q[9];
+    q[TXX] = l2m * (e2[0] * z[0]) + lam * (e2[1] * z[1] + e2[2] * z[2]);
+    q[TYY] = l2m * (e2[1] * z[1]) + lam * (e2[0] * z[0] + e2[2] * z[2]);
+    q[TZZ] = l2m * (e2[2] * z[2]) + lam * (e2[0] * z[0] + e2[1] * z[1]);
+    q[TXY] = mu * (e2[1] * z[0] + e2[0] * z[1]);
+    q[TXZ] = mu * (e2[2] * z[0] + e2[0] * z[2]);
+    q[TYZ] = mu * (e2[2] * z[1] + e2[1] * z[2]);
+#pragma unroll
+    for (int c = TXX; c <= TXY; c++) { corr[c] += (cB - 1.0f) * q[c]; ar[c] += cD * q[c]; }
+  }
+#pragma unroll
+  for (int c = 0; c < 9; c++) {
+    const long o = c * P.siz + pa;
+    if (MODE == RK_FIRST) {
+      const float av = __ldg(P.acur + o);
+      P.aout[o] = av + a.ca * ar[c];
+      P.aend[o] = av + a.cb * ar[c];
+    } else if (MODE == RK_MID) {
+      P.aout[o] = __ldg(P.apre + o) + a.ca * ar[c];
+      P.aend[o] += a.cb * ar[c];
+    } else {
+      P.aend[o] += a.cb * ar[c];
+    }
+  }
 }
 
 template <int MODE>
-__device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float h[9]) {
+__device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float v0[9], const float h[9]) {
   const long sc = a.g.scmp;
 #pragma unroll
   for (int c = 0; c < 9; c++) {
     const long o = c * sc + p;
     if (MODE == RK_FIRST) {
-      const float v = __ldg(a.cur + o);
-      a.out[o] = v + a.ca * h[c];
-      a.end[o] = v + a.cb * h[c];
+      a.out[o] = v0[c] + a.ca * h[c];
+      a.end[o] = v0[c] + a.cb * h[c];
     } else if (MODE == RK_MID) {
       a.out[o] = __ldg(a.pre + o) + a.ca * h[c];
       a.end[o] += a.cb * h[c];
@@ -101,20 +187,36 @@ __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float 
 
 enum { INTERIOR = 0, SHELL = 1 };
 
-template <int ID, int JD, int KD, int MODE, int KIND>
-__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 3 : 2) k_volume(const VolArgs a) {
-  const Grid &g = a.g;
-  // locate the box of this block
+// block -> point; boxes with a narrow x extent (PML x slabs) pack their
+// points densely instead of leaving most of a 32-wide row idle
+__device__ __forceinline__ bool locate(const VolArgs &a, int &i, int &j, int &k) {
   int b = 0;
 #pragma unroll 1
   while (b + 1 < a.nbox && (int)blockIdx.x >= a.box[b + 1].first) b++;
   const VolBox &B = a.box[b];
   const int bid = blockIdx.x - B.first;
+  const int ni = B.i1 - B.i0 + 1, nj = B.j1 - B.j0 + 1;
+  if (B.nbx == 0) {
+    // packed: flat index over the (x, y) rectangle of one z row
+    const int t = (bid % B.nby) * (BX * BY) + threadIdx.y * BX + threadIdx.x;
+    k = B.k0 + bid / B.nby;
+    if (t >= ni * nj) return false;
+    i = B.i0 + t % ni;
+    j = B.j0 + t / ni;
+    return true;
+  }
   const int bx = bid % B.nbx, rem = bid / B.nbx, by = rem % B.nby, bz = rem / B.nby;
-  const int i = B.i0 + bx * BX + threadIdx.x;
-  const int j = B.j0 + by * BY + threadIdx.y;
-  const int k = B.k0 + bz;
-  if (i > B.i1 || j > B.j1) return;
+  i = B.i0 + bx * BX + threadIdx.x;
+  j = B.j0 + by * BY + threadIdx.y;
+  k = B.k0 + bz;
+  return i <= B.i1 && j <= B.j1;
+}
+
+template <int ID, int JD, int KD, int MODE, int KIND>
+__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 3 : 2) k_volume(const __grid_constant__ VolArgs a) {
+  const Grid &g = a.g;
+  int i, j, k;
+  if (!locate(a, i, j, k)) return;
   const int I = i + NG, J = j + NG, K = k + NG;
   // split-node slabs (i0-3..i0+3 of unwelded nodes) belong to the fault kernels
   for (int f = 0; f < a.nfault; f++) {
@@ -122,43 +224,76 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 3 : 2) k_volume(co
     if (d >= -3 && d <= 3 && (__ldg(a.fflag[f] + J + (long)K * g.ny) & FL_SPLIT)) return;
   }
   const long p = g.at(I, J, K);
-  const long sy = g.sy, sz = g.sz, sc = g.scmp;
+  const long sc = g.scmp;
   const float *__restrict__ w = a.cur + p;
+  float v0[9];
+#pragma unroll
+  for (int c = 0; c < 9; c++) v0[c] = __ldg(w + c * sc);
   float e[3][3];
 #pragma unroll
   for (int q = 0; q < 9; q++) e[q / 3][q % 3] = __ldg(a.met + (1 + q) * sc + p);
   const float lam = __ldg(a.med + p), mu = __ldg(a.med + sc + p), slw = __ldg(a.med + 2 * sc + p);
   const float l2m = lam + 2.0f * mu;
+  int ox[4], oy[4], oz[4];
+  tap_offsets<ID>(1, ox);
+  tap_offsets<JD>((int)g.sy, oy);
+  tap_offsets<KD>((int)g.sz, oz);
 
   float h[9];
-  float G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
-  float s[3] = { 0.f, 0.f, 0.f };
-  float dvx[3], dvy[3], dvz[3];
-  acc_vel<ID>(w, sc, 1, e[0], G, dvx);
-  acc_stress<ID>(w, sc, 1, e[0], s);
-  acc_vel<JD>(w, sc, sy, e[1], G, dvy);
-  acc_stress<JD>(w, sc, sy, e[1], s);
-  acc_stress<KD>(w, sc, sz, e[2], s);
   if (KIND == INTERIOR) {
-    acc_vel<KD>(w, sc, sz, e[2], G, dvz);
+    float G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
+    float s[3] = { 0.f, 0.f, 0.f };
+    acc_dir<ID>(w, sc, v0, ox, e[0], G, s);
+    acc_dir<JD>(w, sc, v0, oy, e[1], G, s);
+    acc_dir<KD>(w, sc, v0, oz, e[2], G, s);
     h[VX] = slw * s[0]; h[VY] = slw * s[1]; h[VZ] = slw * s[2];
-    hooke(G, lam, mu, l2m, h);
-    rk_update<MODE>(a, p, h);
+    h[TXX] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]);
+    h[TYY] = l2m * G[1][1] + lam * (G[0][0] + G[2][2]);
+    h[TZZ] = l2m * G[2][2] + lam * (G[0][0] + G[1][1]);
+    h[TXY] = mu * (G[0][1] + G[1][0]);
+    h[TXZ] = mu * (G[0][2] + G[2][0]);
+    h[TYZ] = mu * (G[1][2] + G[2][1]);
+    rk_update<MODE>(a, p, v0, h);
     return;
   }
 
   // ---- shell: PML slabs and the rows under the free surface ----------------
   const int nk2 = g.nk + NG - 1;
-  const bool vlow = a.isfree && K >= nk2 - 2;
-  if (!vlow) {
-    acc_vel<KD>(w, sc, sz, e[2], G, dvz);
-    hooke(G, lam, mu, l2m, h);
-  } else {
-    // velocity gradient below the surface: conversion matrices at the
-    // surface, 2nd / 4th order one-sided dz one and two rows below
+  const bool top = a.isfree && K >= nk2 - 3;
+  const bool surfrow = a.isfree && K == nk2;
+  const long fidx = ((long)J * g.nx + I) * 9;
+  float corr[9], r[9], D[9], dvx[3], dvy[3];
+#pragma unroll
+  for (int c = 0; c < 9; c++) corr[c] = 0.f;
+  // x
+  derivs<ID>(w, sc, v0, ox, D);
+  dvx[0] = D[VX]; dvx[1] = D[VY]; dvx[2] = D[VZ];
+  rhs_dir(D, e[0], lam, mu, l2m, slw, r);
+#pragma unroll
+  for (int c = 0; c < 9; c++) h[c] = r[c];
+  if (a.pml[0].on) pml_face<MODE>(a, a.pml[0], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  if (a.pml[1].on) pml_face<MODE>(a, a.pml[1], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  // y
+  derivs<JD>(w, sc, v0, oy, D);
+  dvy[0] = D[VX]; dvy[1] = D[VY]; dvy[2] = D[VZ];
+  rhs_dir(D, e[1], lam, mu, l2m, slw, r);
+#pragma unroll
+  for (int c = 0; c < 9; c++) h[c] += r[c];
+  if (a.pml[2].on) pml_face<MODE>(a, a.pml[2], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  if (a.pml[3].on) pml_face<MODE>(a, a.pml[3], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  // z
+  derivs<KD>(w, sc, v0, oz, D);
+  rhs_dir(D, e[2], lam, mu, l2m, slw, r);
+  if (a.pml[4].on) pml_face<MODE>(a, a.pml[4], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
+  if (a.pml[5].on) pml_face<MODE>(a, a.pml[5], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
+  if (top && K >= nk2 - 2) {
+    // velocity below the surface: the z part of the velocity gradient comes
+    // from the conversion matrices (surface) or from 2nd / 4th order
+    // one-sided differences (one / two rows below)
+    const long sz = g.sz;
     float dz[3];
     if (K == nk2) {
-      const float *X = a.free_mat + ((long)J * g.nx + I) * 9;
+      const float *X = a.free_mat + fidx;
       const float *Y = X + (long)g.ny * g.nx * 9;
       float o1[3], o2[3];
       mv3(X, dvx, o1); mv3(Y, dvy, o2);
@@ -168,112 +303,45 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 3 : 2) k_volume(co
     } else {
       dz[0] = mac24(w + VX * sc, sz, KD); dz[1] = mac24(w + VY * sc, sz, KD); dz[2] = mac24(w + VZ * sc, sz, KD);
     }
+    float Dz[9], rz[9];
 #pragma unroll
-    for (int c = 0; c < 3; c++)
+    for (int c = 0; c < 9; c++) Dz[c] = 0.f;
+    Dz[VX] = dz[0]; Dz[VY] = dz[1]; Dz[VZ] = dz[2];
+    rhs_dir(Dz, e[2], lam, mu, l2m, slw, rz);
 #pragma unroll
-      for (int bb = 0; bb < 3; bb++) G[c][bb] += e[2][bb] * dz[c];
-    hooke(G, lam, mu, l2m, h);
+    for (int c = TXX; c <= TXY; c++) h[c] += rz[c];
+#pragma unroll
+    for (int c = VX; c <= VZ; c++) h[c] += r[c];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 9; c++) h[c] += r[c];
   }
-  h[VX] = slw * s[0]; h[VY] = slw * s[1]; h[VZ] = slw * s[2];
-  if (a.isfree && K >= nk2 - (KD ? 3 : 1)) {
+  if (top && K >= nk2 - (KD ? 3 : 1)) {
     // traction image on the momentum equation in the top rows
     const float *cur = a.cur;
+    const long sy = g.sy;
     const float sj = slw / __ldg(a.met + MJAC * sc + p);
 #pragma unroll 1
-    for (int r = 0; r < 3; r++) {
+    for (int rr = 0; rr < 3; rr++) {
       float dx = 0.f, dy = 0.f, dzz = 0.f;
 #pragma unroll
-      for (int n = 0; n < 5; n++) {
-        const int o = ID ? n - 1 : n - 3;
-        dx += drp_w(ID, n) * ctrac(cur, a.met, sc, p + o, MXIX, r);
-      }
+      for (int n = 0; n < 5; n++) dx += wdrp<ID>(n) * ctrac(cur, a.met, sc, p + (ID ? n - 1 : n - 3), MXIX, rr);
 #pragma unroll
-      for (int n = 0; n < 5; n++) {
-        const int o = JD ? n - 1 : n - 3;
-        dy += drp_w(JD, n) * ctrac(cur, a.met, sc, p + o * sy, METX, r);
-      }
+      for (int n = 0; n < 5; n++) dy += wdrp<JD>(n) * ctrac(cur, a.met, sc, p + (JD ? n - 1 : n - 3) * sy, METX, rr);
 #pragma unroll
       for (int n = 0; n < 5; n++) {
         const int kk = K + (KD ? n - 1 : n - 3);
         float v = 0.f;
-        if (kk < nk2) v = ctrac(cur, a.met, sc, g.at(I, J, kk), MZTX, r);
-        else if (kk > nk2) v = -ctrac(cur, a.met, sc, g.at(I, J, 2 * nk2 - kk), MZTX, r);
-        dzz += drp_w(KD, n) * v;
+        if (kk < nk2) v = ctrac(cur, a.met, sc, g.at(I, J, kk), MZTX, rr);
+        else if (kk > nk2) v = -ctrac(cur, a.met, sc, g.at(I, J, 2 * nk2 - kk), MZTX, rr);
+        dzz += wdrp<KD>(n) * v;
       }
-      h[VX + r] = (dx + dy + dzz) * sj;
+      h[VX + rr] = (dx + dy + dzz) * sj;
     }
   }
-
-  // CFS-PML: faces add up where they overlap
 #pragma unroll
-  for (int fc = 0; fc < 6; fc++) {
-    const int d = fc >> 1;
-    const PmlFaceDev &P = a.pml[fc];
-    if (!P.on) continue;
-    const int li = I - P.i1, lj = J - P.j1, lk = K - P.k1;
-    if (li < 0 || li >= P.fni || lj < 0 || lj >= P.fnj || lk < 0 || lk >= P.fnk) continue;
-    const int layer = d == 0 ? li : (d == 1 ? lj : lk);
-    const float cA = __ldg(P.A + layer), cB = __ldg(P.B + layer), cD = __ldg(P.D + layer);
-    const float ex = e[d][0], ey = e[d][1], ez = e[d][2];
-    const int DF = d == 0 ? ID : (d == 1 ? JD : KD);
-    const long st = d == 0 ? 1 : (d == 1 ? sy : sz);
-    float Dd[9];
-#pragma unroll
-    for (int c = 0; c < 9; c++) Dd[c] = DF ? drp<1>(w + c * sc, st) : drp<0>(w + c * sc, st);
-    float r[9];
-    r[VX] = slw * (ex * Dd[TXX] + ey * Dd[TXY] + ez * Dd[TXZ]);
-    r[VY] = slw * (ex * Dd[TXY] + ey * Dd[TYY] + ez * Dd[TYZ]);
-    r[VZ] = slw * (ex * Dd[TXZ] + ey * Dd[TYZ] + ez * Dd[TZZ]);
-    r[TXX] = l2m * ex * Dd[VX] + lam * ey * Dd[VY] + lam * ez * Dd[VZ];
-    r[TYY] = lam * ex * Dd[VX] + l2m * ey * Dd[VY] + lam * ez * Dd[VZ];
-    r[TZZ] = lam * ex * Dd[VX] + lam * ey * Dd[VY] + l2m * ez * Dd[VZ];
-    r[TXY] = mu * (ey * Dd[VX] + ex * Dd[VY]);
-    r[TXZ] = mu * (ez * Dd[VX] + ex * Dd[VZ]);
-    r[TYZ] = mu * (ez * Dd[VY] + ey * Dd[VZ]);
-    const long pa = li + (long)lj * P.fni + (long)lk * P.fni * P.fnj;
-    const float *ac = P.acur + pa;
-    float ar[9];
-#pragma unroll
-    for (int c = 0; c < 9; c++) {
-      const float av = __ldg(ac + c * P.siz);
-      h[c] += (cB - 1.0f) * r[c] - cB * av;
-      ar[c] = cD * r[c] - cA * av;
-    }
-    if (d < 2 && a.isfree && K == nk2) {
-      // free-surface coupling of the x / y faces: the d-derivative of the
-      // surface-converted dz velocity gradient
-      const float *X = a.free_mat + (long)(d == 0 ? 0 : 1) * g.ny * g.nx * 9 + ((long)J * g.nx + I) * 9;
-      const float dd[3] = { Dd[VX], Dd[VY], Dd[VZ] };
-      float z[3];
-      mv3(X, dd, z);
-      const float zx = e[2][0], zy = e[2][1], zz = e[2][2];
-      float q[9];
-      q[TXX] = l2m * (zx * z[0]) + lam * (zy * z[1] + zz * z[2]);
-      q[TYY] = l2m * (zy * z[1]) + lam * (zx * z[0] + zz * z[2]);
-      q[TZZ] = l2m * (zz * z[2]) + lam * (zx * z[0] + zy * z[1]);
-      q[TXY] = mu * (zy * z[0] + zx * z[1]);
-      q[TXZ] = mu * (zz * z[0] + zx * z[2]);
-      q[TYZ] = mu * (zz * z[1] + zy * z[2]);
-#pragma unroll
-      for (int c = TXX; c <= TXY; c++) { h[c] += (cB - 1.0f) * q[c]; ar[c] += cD * q[c]; }
-    }
-    float *aE = P.aend + pa;
-#pragma unroll
-    for (int c = 0; c < 9; c++) {
-      const long o = c * P.siz;
-      if (MODE == RK_FIRST) {
-        const float av = __ldg(ac + o);
-        P.aout[pa + o] = av + a.ca * ar[c];
-        aE[o] = av + a.cb * ar[c];
-      } else if (MODE == RK_MID) {
-        P.aout[pa + o] = __ldg(P.apre + pa + o) + a.ca * ar[c];
-        aE[o] += a.cb * ar[c];
-      } else {
-        aE[o] += a.cb * ar[c];
-      }
-    }
-  }
-  rk_update<MODE>(a, p, h);
+  for (int c = 0; c < 9; c++) h[c] += corr[c];
+  rk_update<MODE>(a, p, v0, h);
 }
 
 template <int ID, int JD, int KD, int KIND>
@@ -302,7 +370,8 @@ void launch_kind(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaS
 
 }  // namespace
 
-// boxes (interior indices, inclusive) -> block layout of one launch
+// boxes (interior indices, inclusive) -> block layout of one launch; boxes
+// at most 24 points wide in x are packed (nbx = 0)
 void volume_boxes(VolArgs &a, const int (*boxes)[6], int n) {
   a.nbox = 0;
   int first = 0;
@@ -311,10 +380,18 @@ void volume_boxes(VolArgs &a, const int (*boxes)[6], int n) {
     if (b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) continue;
     VolBox &B = a.box[a.nbox++];
     B.i0 = b[0]; B.i1 = b[1]; B.j0 = b[2]; B.j1 = b[3]; B.k0 = b[4];
-    B.nbx = (b[1] - b[0] + BX) / BX;
-    B.nby = (b[3] - b[2] + BY) / BY;
-    B.first = first;
-    first += B.nbx * B.nby * (b[5] - b[4] + 1);
+    const int ni = b[1] - b[0] + 1, nj = b[3] - b[2] + 1, nk = b[5] - b[4] + 1;
+    if (ni <= 24) {
+      B.nbx = 0;
+      B.nby = (ni * nj + BX * BY - 1) / (BX * BY);
+      B.first = first;
+      first += B.nby * nk;
+    } else {
+      B.nbx = (ni + BX - 1) / BX;
+      B.nby = (nj + BY - 1) / BY;
+      B.first = first;
+      first += B.nbx * B.nby * nk;
+    }
   }
   a.nblocks = first;
 }
