@@ -16,7 +16,7 @@ LIB = os.path.join(LIBDIR, "libcgfd.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 
-CU = ["volume.cu", "volume_tiled.cu", "volume_tma.cu", "fault.cu", "api.cu"]
+CU = ["volume.cu", "volume_zq.cu", "volume_tiled.cu", "volume_tma.cu", "fault.cu", "api.cu"]
 CPP = ["setup.cpp"]
 HEADERS = ["common.h", "ops.cuh", "setup.h"]
 

@@ -25,11 +25,13 @@ void launch_volume(const VolArgs &interior, const VolArgs &shell, int idir, int 
                    cudaStream_t st);
 void volume_boxes(VolArgs &a, const int (*boxes)[6], int n);
 void launch_volume_tiled(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void volume_zq_layout(VolArgs &a, const int box[6], int kchunk);
+void launch_volume_zq(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void volume_tma_prepare();
 int volume_tma_encode(CUtensorMap *tm, const float *level, const Grid &g);
 void launch_volume_tma(const CUtensorMap &tm, const VolArgs &a, int idir, int jdir, int kdir, int mode,
                        cudaStream_t st);
-void launch_fault_stage(const FaultArgs &a, cudaStream_t st);
+int launch_fault_stage(const FaultArgs &a, cudaStream_t st);
 void launch_record(const StationArgs &a, cudaStream_t st);
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
 }  // namespace cgfd
@@ -52,6 +54,7 @@ struct FaultState {
   float *lev[4] = {};                   // storage slots, [9][2][ny*nz]
   uint8_t *flag = nullptr;
   float *mat = nullptr, *fmat = nullptr, *scal = nullptr, *out = nullptr;
+  float *trac = nullptr;                // traction scratch of the split box
 };
 
 struct PmlState {
@@ -86,7 +89,8 @@ struct cgfd_solver {
   long long vol_launches = 0;
   int it = 0;
   long long launches_per_step = 0, last_launches = 0;
-  int tiled = 2, kchunk = 32;           // volume kernel: 2 TMA-fed, 1 smem-tiled, 0 boxes
+  int tiled = 0, kchunk = 32;           // volume kernel: 0 boxes, 1 smem-tiled, 2 TMA-fed, 3 z-marching interior + boxes
+  int kchunk_zq = 32;
   int kchunk_tma = 32;
   int box_top[1][6];                    // rows under the free surface
   CUtensorMap tmap[4];                  // TMA maps of the 4 level slots
@@ -152,8 +156,8 @@ void enqueue_step(cgfd_solver *s, int it) {
       a.ca = ca; a.cb = cb; a.rkb = kRkB[stage]; a.dt = s->dt;
       a.isfree = s->isfree; a.imethod = s->imethod;
       a.j0 = F.j0; a.k0 = F.k0; a.nj = F.nj; a.nk = F.nk; a.ctl = s->ctl;
-      launch_fault_stage(a, s->stream);
-      nl += (F.nj > 0 && F.nk > 0) ? 3 : 1;
+      a.trac = F.trac; a.tj0 = F.j0 + NG - 3; a.tk0 = F.k0 + NG - 3; a.tnj = F.nj + 6; a.tnk = F.nk + 6;
+      nl += launch_fault_stage(a, s->stream);
     }
     VolArgs v{};
     v.g = s->g; v.cur = s->w[scur]; v.pre = s->w[spre]; v.out = sout >= 0 ? s->w[sout] : nullptr; v.end = s->w[send];
@@ -184,16 +188,27 @@ void enqueue_step(cgfd_solver *s, int it) {
       VolArgs none = vs;
       none.nbox = 0;
       launch_volume(none, vs, idir, jdir, kdir, mode, s->stream);
+      nl += 1 + (vs.nbox > 0);
     } else if (s->tiled == 1) {
       launch_volume_tiled(v, idir, jdir, kdir, mode, s->stream);
-      vi.nbox = 1; vs.nbox = 0;
+      nl += 1;
+    } else if (s->tiled == 3) {
+      // interior box: z-marching kernel; PML slabs and surface rows: boxes
+      VolArgs vz = v;
+      volume_zq_layout(vz, s->box_in[0], s->kchunk_zq);
+      launch_volume_zq(vz, idir, jdir, kdir, mode, s->stream);
+      volume_boxes(vs, s->box_shell, 6);
+      VolArgs none = vs;
+      none.nbox = 0;
+      launch_volume(none, vs, idir, jdir, kdir, mode, s->stream);
+      nl += (vz.nbox > 0) + (vs.nbox > 0);
     } else {
       volume_boxes(vi, s->box_in, 1);
       volume_boxes(vs, s->box_shell, 6);
       launch_volume(vi, vs, idir, jdir, kdir, mode, s->stream);
+      nl += (vi.nbox > 0) + (vs.nbox > 0);
     }
     if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
-    nl += (vi.nbox > 0) + (vs.nbox > 0) + (s->tiled ? 1 : 0);
   }
   launch_advance(s->ctl, s->st.max_rec, s->stream);
   nl++;
@@ -290,6 +305,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   s->tiled = 0;
   if (vk && std::strcmp(vk, "tma") == 0) s->tiled = 2;
   if (vk && std::strcmp(vk, "tiled") == 0) s->tiled = 1;
+  if (vk && std::strcmp(vk, "zq") == 0) s->tiled = 3;
   {
     // z chunk per block: enough blocks for several waves, rows >= 8
     const long bxy = (long)((H.g.ni + 31) / 32) * ((H.g.nj + 7) / 8);
@@ -352,7 +368,10 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
       if (Fh.flag[(size_t)(j + NG) + (size_t)(k + NG) * g.ny] & FL_SPLIT) {
         j0 = std::min(j0, j); j1 = std::max(j1, j); k0 = std::min(k0, k); k1 = std::max(k1, k);
       }
-    if (j1 >= 0) { F.j0 = j0; F.k0 = k0; F.nj = j1 - j0 + 1; F.nk = k1 - k0 + 1; }
+    if (j1 >= 0) {
+      F.j0 = j0; F.k0 = k0; F.nj = j1 - j0 + 1; F.nk = k1 - k0 + 1;
+      CK(dalloc(s, &F.trac, (size_t)12 * 9 * (F.nj + 6) * (F.nk + 6)), "fault traction scratch");
+    }
     s->faults.push_back(F);
   }
   // stations
@@ -393,6 +412,17 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     std::memcpy(s->box_shell, sh, sizeof sh);
     const int bt[6] = { 0, g.ni - 1, 0, g.nj - 1, s->isfree ? g.nk - 4 : g.nk, g.nk - 1 };
     std::memcpy(s->box_top[0], bt, sizeof bt);
+    // z chunk of the z-marching kernel: about 8 waves of 2 blocks per SM
+    // over the interior box's 32 x 8 tiles, at least 16 rows per chunk
+    int nsm = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long tiles = (long)((ihi - ilo + 32) / 32) * ((jhi - jlo + 8) / 8);
+    const long nz = std::max(1, khi - klo + 1);
+    const long nch = std::max<long>(1, (8L * 2 * nsm + tiles - 1) / std::max<long>(1, tiles));
+    s->kchunk_zq = (int)std::max<long>(16, (nz + nch - 1) / nch);
+    const char *kc = std::getenv("CGFD_ZQ_KCHUNK");
+    if (kc && std::atoi(kc) > 0) s->kchunk_zq = std::atoi(kc);
   }
   CK(dalloc(s, &s->ctl, 1), "control block");
   for (int q = 0; q < 2; q++) CK(cudaEventCreate(&s->ev_run[q]), "event");

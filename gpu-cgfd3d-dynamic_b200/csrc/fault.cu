@@ -1,31 +1,42 @@
-// fault.cu -- split-node fault kernels, one thread per fault node.
+// fault.cu -- split-node fault kernels.
 //
 // Per RK stage the reference launches, per fault, wave2fault, the trial
 // traction + slip-weakening friction kernel, fault2wave, the fault velocity
 // RHS, the fault stress RHS (forward or backward variant), two fault RK
 // updates, fault2wave again and the stage traction update, each as its own
-// kernel (src/forward/drv_rk_curv_col.cu:277-588).  Here that becomes three
+// kernel (src/forward/drv_rk_curv_col.cu:277-588).  Here that becomes five
 // kernels over the fault plane:
 //
 //   k_fault_weld    welded nodes: fault wavefield from the volume at i0
 //                   (wave2fault_gpu, src/forward/transform.cu:101-212)
-//   k_fault_vel     split nodes: T1 traction image, trial traction and
-//                   linear slip-weakening friction (trial_slipweakening_gpu,
-//                   src/forward/trial_slipweakening.cu:92-388), velocity RHS
-//                   at i0-3..i0+3 and at both split nodes
-//                   (sv_curv_col_el_iso_rhs_fault_velo_gpu,
-//                   src/forward/sv_curv_col_el_iso_fault_gpu.cu:192-429),
-//                   RK update of those velocities, stage traction output
-//                   (fault_var_stage_update_gpu, fault_wav_t.cu:291-316)
-//   k_fault_stress  split nodes: stress RHS at i0-3..i0+3 and fault traction
-//                   rates (..._stress_F_gpu :432-1159 / _B_gpu :1162-1879),
-//                   RK update, then the split-node volume point from the
-//                   fault fields (fault2wave_gpu, transform.cu:293-376) and,
-//                   after the last stage, slip / slip rate / rupture time
-//                   (fault_var_update_gpu, fault_wav_t.cu:198-264)
+//   k_fault_trac    tractions J e . sigma of the stage input at the volume
+//                   points i0-6..i0+6 around the split box, once each, into a
+//                   per-fault scratch array read by the next two kernels
+//   k_fault_trial   split nodes, one thread each: T1 traction image, trial
+//                   traction and linear slip-weakening friction
+//                   (trial_slipweakening_gpu,
+//                   src/forward/trial_slipweakening.cu:92-388), stage
+//                   traction output (fault_var_stage_update_gpu,
+//                   fault_wav_t.cu:291-316), split-node velocity RHS
+//                   (sv_curv_col_el_iso_fault_gpu.cu:323-429) and its RK update
+//   k_fault_vslab   velocity RHS and RK update at i0-3..i0+3, one thread per
+//                   volume point (sv_curv_col_el_iso_rhs_fault_velo_gpu,
+//                   src/forward/sv_curv_col_el_iso_fault_gpu.cu:192-322)
+//   k_fault_sslab   stress RHS and RK update at i0-3..i0+3, one thread per
+//                   volume point (..._stress_F_gpu :432-1159 / _B_gpu
+//                   :1162-1879)
+//   k_fault_node    split nodes, one thread each: fault traction rates of
+//                   both sides and their RK update, the split-node volume
+//                   point from the fault fields (fault2wave_gpu,
+//                   transform.cu:293-376) and, after the last stage, slip /
+//                   slip rate / rupture time (fault_var_update_gpu,
+//                   fault_wav_t.cu:198-264)
 //
 // The volume stage kernel skips i0-3..i0+3 of split nodes, so these kernels
-// own those points' RK update.  Fault-plane work is a few percent of a step.
+// own those points' RK update.  The slab and traction kernels give each
+// (node, x offset) its own thread with the x offset fastest: the fault plane
+// is a constant-x plane, so a warp over nodes alone would touch one cache
+// line per thread on every volume access.
 #include <cuda_runtime.h>
 
 #include "ops.cuh"
@@ -48,21 +59,34 @@ __device__ __forceinline__ void trac3(const float *__restrict__ w, const float *
   t[2] = J * (ex * sxz + ey * syz + ez * szz);
 }
 
-// stage update of one value: first stage (out, end from the input), middle
-// stages (out from P, end accumulates), last stage (end accumulates)
-__device__ __forceinline__ void rk_put(int mode, float ca, float cb, const float *cur, const float *pre,
-                                       float *out, float *end, long o, float h) {
+// stage update of N values; every level read is issued before the first
+// store (the compiler cannot prove that the levels do not alias, and
+// interleaved load / store pairs cost one memory round trip each)
+template <int N>
+__device__ __forceinline__ void rk_put_n(int mode, float ca, float cb, const float *cur, const float *pre,
+                                         float *out, float *end, const long o[N], const float h[N]) {
+  float u[N], e[N];
   if (mode == RK_FIRST) {
-    const float v = cur[o];
-    out[o] = v + ca * h;
-    end[o] = v + cb * h;
-  } else if (mode == RK_MID) {
-    out[o] = pre[o] + ca * h;
-    end[o] += cb * h;
+#pragma unroll
+    for (int n = 0; n < N; n++) u[n] = cur[o[n]];
+#pragma unroll
+    for (int n = 0; n < N; n++) { out[o[n]] = u[n] + ca * h[n]; end[o[n]] = u[n] + cb * h[n]; }
   } else {
-    end[o] += cb * h;
+#pragma unroll
+    for (int n = 0; n < N; n++) {
+      if (mode == RK_MID) u[n] = pre[o[n]];
+      e[n] = end[o[n]];
+    }
+#pragma unroll
+    for (int n = 0; n < N; n++) {
+      if (mode == RK_MID) out[o[n]] = u[n] + ca * h[n];
+      end[o[n]] = e[n] + cb * h[n];
+    }
   }
 }
+
+// slot of x offset d (-6..-1, 1..6) in the traction scratch
+__device__ __forceinline__ int trac_slot(int d) { return d < 0 ? d + 6 : d + 5; }
 
 // split-node volume point from the fault fields (fault2wave_gpu,
 // transform.cu:293-376): velocity = mean of the two sides, stress from the
@@ -137,7 +161,40 @@ __global__ void k_fault_weld(const FaultArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_fault_vel(const FaultArgs a) {
+// tractions of the stage input around the split box, one thread per
+// (node, x offset), x offset fastest so that a warp reads contiguous x runs:
+// T1 = J e_xi . sigma at x = i0+-1..6, T2 = J e_eta . sigma and
+// T3 = J e_zeta . sigma at x = i0+-1..3.  The trial, friction and slab
+// velocity kernels read them from here instead of recomputing each one
+// (10 loads) for every tap.  Layout [9][tnk][tnj][12], x offset fastest.
+__global__ void __launch_bounds__(192) k_fault_trac(const FaultArgs a) {
+  const Grid &g = a.g;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long node = t / 12;
+  if (node >= (long)a.tnj * a.tnk) return;
+  const int slot = (int)(t - node * 12);
+  const int d = slot < 6 ? slot - 6 : slot - 5;
+  const int kk = (int)(node / a.tnj), jj = (int)(node - (long)kk * a.tnj);
+  const long sc = g.scmp, pl = (long)a.tnj * a.tnk * 12;
+  const long q = g.at(a.F.i0 + d, a.tj0 + jj, a.tk0 + kk);
+  float *tp = a.trac + node * 12 + slot;
+  float v[3];
+  trac3(a.wcur, a.met, sc, q, MXIX, v);
+  tp[0] = v[0]; tp[pl] = v[1]; tp[2 * pl] = v[2];
+  if (d >= -3 && d <= 3) {
+    trac3(a.wcur, a.met, sc, q, METX, v);
+    tp[3 * pl] = v[0]; tp[4 * pl] = v[1]; tp[5 * pl] = v[2];
+    trac3(a.wcur, a.met, sc, q, MZTX, v);
+    tp[6 * pl] = v[0]; tp[7 * pl] = v[1]; tp[8 * pl] = v[2];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// split nodes, one thread per node: trial traction and linear slip-weakening
+// friction (trial_slipweakening_gpu), the stage traction output, the refresh
+// of the stage input's split-node volume point, and the split-node velocity
+// RHS with its RK update
+__global__ void __launch_bounds__(128) k_fault_trial(const FaultArgs a) {
   const Grid &g = a.g;
   const int j = a.j0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int k = a.k0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -148,19 +205,22 @@ __global__ void __launch_bounds__(128) k_fault_vel(const FaultArgs a) {
   const uint8_t fl = F.flag[nd];
   if (!(fl & FL_SPLIT)) return;
   const int i0 = F.i0;
-  const float *w = a.wcur, *met = a.met;
+  const float *met = a.met;
   const long ny = g.ny;
   const int km = g.nk - (k + 1);
   const bool surf = a.isfree && km <= 3;
   const int nf = km + 3;
 
-  // T1 = J e_xi . sigma along x through the split node, i0-6..i0+6 (index 6
-  // is the split node, filled after the friction law)
-  float X1[13][3];
+  // T1 = J e_xi . sigma at i0-3..i0+3 (index 3 is the split node, filled
+  // after the friction law)
+  float X1[7][3];
+  const long pl = (long)a.tnj * a.tnk * 12;
+  const float *tr = a.trac + ((long)(K - a.tk0) * a.tnj + (J - a.tj0)) * 12;
 #pragma unroll
-  for (int l = -6; l <= 6; l++) {
+  for (int l = -3; l <= 3; l++) {
     if (l == 0) continue;
-    trac3(w, met, sc, g.at(i0 + l, J, K), MXIX, X1[l + 6]);
+#pragma unroll
+    for (int c = 0; c < 3; c++) X1[l + 3][c] = tr[c * pl + trac_slot(l)];
   }
 
   // along-fault derivatives of the fault tractions, both sides
@@ -186,7 +246,7 @@ __global__ void __launch_bounds__(128) k_fault_vel(const FaultArgs a) {
       }
       DzT3[m][c] = dz;
       const int s = 2 * m - 1;
-      const float img = kA1 * X1[6 + s][c] + kA2 * X1[6 + 2 * s][c] + kA3 * X1[6 + 3 * s][c];
+      const float img = kA1 * X1[3 + s][c] + kA2 * X1[3 + 2 * s][c] + kA3 * X1[3 + 3 * s][c];
       R[m][c] = 0.5f * ((float)s * img + (DyT2[m][c] + DzT3[m][c]));
     }
   }
@@ -233,10 +293,10 @@ __global__ void __launch_bounds__(128) k_fault_vel(const FaultArgs a) {
     for (int c = 0; c < 3; c++) { Tau[c] = Tl[c]; T1s[c] = Tr[c]; }
   }
 #pragma unroll
-  for (int c = 0; c < 3; c++) { F.scal[(FS_T1X + c) * ns + nd] = T1s[c]; X1[6][c] = T1s[c]; }
+  for (int c = 0; c < 3; c++) { F.scal[(FS_T1X + c) * ns + nd] = T1s[c]; X1[3][c] = T1s[c]; }
   // the stage input level sees the new split-node traction before the volume
-  // kernel reads it (drv_rk_curv_col.cu:285, fault2wave on w_cur); this
-  // kernel never reads the volume at i0 itself
+  // kernel reads it (drv_rk_curv_col.cu:285, fault2wave on w_cur); no fault
+  // kernel reads the volume at i0
   split_to_volume(g, met, sc, ns, nd, i0, J, K, a.fc, T1s, const_cast<float *>(a.wcur));
   {
     const float s1[3] = { F.scal[FS_S1X * ns + nd], F.scal[FS_S1Y * ns + nd], F.scal[FS_S1Z * ns + nd] };
@@ -248,61 +308,203 @@ __global__ void __launch_bounds__(128) k_fault_vel(const FaultArgs a) {
     else { *Tn += a.rkb * Tau_n; *T1o += a.rkb * tTs1; *T2o += a.rkb * tTs2; }
   }
 
-  // velocity RHS at i0+s, s = -3..3 (s != 0)
-#pragma unroll
-  for (int s = -3; s <= 3; s++) {
-    if (s == 0) continue;
-    const long q = g.at(i0 + s, J, K);
-    float hv[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      float v1[7];
-#pragma unroll
-      for (int l = 0; l < 7; l++) v1[l] = X1[6 + s + l - 3][c];
-      // odd extension of T1 through the split node (Zhang's traction image)
-      if (s == -2) { v1[6] = 2.f * v1[5] - v1[4]; }
-      if (s == -1) { v1[5] = 2.f * v1[4] - v1[3]; v1[6] = 2.f * v1[4] - v1[2]; }
-      if (s == 1) { v1[0] = 2.f * v1[2] - v1[4]; v1[1] = 2.f * v1[2] - v1[3]; }
-      if (s == 2) { v1[0] = 2.f * v1[1] - v1[2]; }
-      hv[c] = drp_v(v1 + 3, a.idir);
-    }
-    float v2[7][3], v3[7][3];
-#pragma unroll
-    for (int l = 0; l < 7; l++) {
-      trac3(w, met, sc, q + (long)(l - 3) * g.sy, METX, v2[l]);
-      trac3(w, met, sc, q + (long)(l - 3) * g.sz, MZTX, v3[l]);
-    }
-    const float rr = __ldg(a.med + 2 * sc + q) / __ldg(met + MJAC * sc + q);
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      float y[7], z[7];
-#pragma unroll
-      for (int l = 0; l < 7; l++) { y[l] = v2[l][c]; z[l] = v3[l][c]; }
-      if (surf) {
-        z[nf] = 0.f;
-        for (int l = nf + 1; l < 7; l++) z[l] = -z[2 * nf - l];
-      }
-      const float h = (hv[c] + drp_v(y + 3, a.jdir) + drp_v(z + 3, a.kdir)) * rr;
-      rk_put(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, (VX + c) * sc + q, h);
-    }
-  }
-
-  // split-node velocity RHS and RK update
+  // split-node velocity RHS and RK update (the output levels only; the
+  // stress kernel of this stage reads the fault velocity of the input level)
+  long o[6];
+  float hv[6];
 #pragma unroll
   for (int m = 0; m < 2; m++) {
     const float rr = 1.0f / ((m ? rho1 : rho0) * jac0);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const float dx = m == 0 ? (kA0 * X1[6][c] - kA1 * X1[5][c] - kA2 * X1[4][c] - kA3 * X1[3][c])
-                              : (-kA0 * X1[6][c] + kA1 * X1[7][c] + kA2 * X1[8][c] + kA3 * X1[9][c]);
-      const float h = (dx + DyT2[m][c] + DzT3[m][c]) * rr;
-      rk_put(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, fidx(FVX + c, m, ns, nd), h);
+      const float dx = m == 0 ? (kA0 * X1[3][c] - kA1 * X1[2][c] - kA2 * X1[1][c] - kA3 * X1[0][c])
+                              : (-kA0 * X1[3][c] + kA1 * X1[4][c] + kA2 * X1[5][c] + kA3 * X1[6][c]);
+      hv[3 * m + c] = (dx + DyT2[m][c] + DzT3[m][c]) * rr;
+      o[3 * m + c] = fidx(FVX + c, m, ns, nd);
     }
   }
+  rk_put_n<6>(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, o, hv);
+}
+
+// x offset from the fault of slab slot y = 0..5: -3, -2, -1, 1, 2, 3
+__device__ __forceinline__ int slab_offset(int y) { return y < 3 ? y - 3 : y - 2; }
+
+// slab work item t over the split box, six per node with the x offset
+// fastest (a warp reads runs of contiguous x): node (j, k), offset s
+__device__ __forceinline__ bool slab_item(const FaultArgs &a, long t, int &j, int &k, int &s) {
+  const long node = t / 6;
+  if (node >= (long)a.nj * a.nk) return false;
+  const int r = (int)(t - node * 6);
+  k = a.k0 + (int)(node / a.nj);
+  j = a.j0 + (int)(node - (long)(k - a.k0) * a.nj);
+  s = slab_offset(r);
+  return true;
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_fault_stress(const FaultArgs a) {
+// velocity RHS at the six volume points i0-3..i0+3 (not i0) of split nodes,
+// one thread per point, one warp per (slab offset, row of 32 nodes)
+// (sv_curv_col_el_iso_rhs_fault_velo_gpu, :192-322)
+__global__ void __launch_bounds__(192) k_fault_vslab(const FaultArgs a) {
+  const Grid &g = a.g;
+  int j, k, s;
+  if (!slab_item(a, (long)blockIdx.x * blockDim.x + threadIdx.x, j, k, s)) return;
+  const int J = j + NG, K = k + NG;
+  const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny, sc = g.scmp;
+  const FaultDev &F = a.F;
+  if (!(F.flag[nd] & FL_SPLIT)) return;
+  const int i0 = F.i0;
+  const int km = g.nk - (k + 1);
+  const bool surf = a.isfree && km <= 3;
+  const int nf = km + 3;
+  const long q = g.at(i0 + s, J, K);
+  const long pl = (long)a.tnj * a.tnk * 12, row = (long)a.tnj * 12;
+  const float *tr = a.trac + ((long)(K - a.tk0) * a.tnj + (J - a.tj0)) * 12;
+
+  // T1 along x through this point: this side's volume points, the split
+  // node's T1 at the fault, and beyond it the odd extension through the
+  // split node (traction image)
+  float v1[7][3];
+#pragma unroll
+  for (int l = -3; l <= 3; l++) {
+    const int x = s + l;
+    if (x == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) v1[l + 3][c] = F.scal[(FS_T1X + c) * ns + nd];
+    } else if ((x < 0) == (s < 0)) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) v1[l + 3][c] = tr[c * pl + trac_slot(x)];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; c++) v1[l + 3][c] = 0.f;
+    }
+  }
+  float hv[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float v[7];
+#pragma unroll
+    for (int l = 0; l < 7; l++) v[l] = v1[l][c];
+    if (s == -2) { v[6] = 2.f * v[5] - v[4]; }
+    if (s == -1) { v[5] = 2.f * v[4] - v[3]; v[6] = 2.f * v[4] - v[2]; }
+    if (s == 1) { v[0] = 2.f * v[2] - v[4]; v[1] = 2.f * v[2] - v[3]; }
+    if (s == 2) { v[0] = 2.f * v[1] - v[2]; }
+    hv[c] = drp_v(v + 3, a.idir);
+  }
+
+  // y and z lines of T2 = J e_eta . sigma and T3 = J e_zeta . sigma
+  const float *t2 = tr + 3 * pl + trac_slot(s), *t3 = t2 + 3 * pl;
+  const float rr = __ldg(a.med + 2 * sc + q) / __ldg(a.met + MJAC * sc + q);
+  long o[3];
+  float h[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float y[7], z[7];
+#pragma unroll
+    for (int l = 0; l < 7; l++) {
+      y[l] = t2[c * pl + (l - 3) * 12];
+      z[l] = t3[c * pl + (l - 3) * row];
+    }
+    if (surf) {
+      z[nf] = 0.f;
+      for (int l = nf + 1; l < 7; l++) z[l] = -z[2 * nf - l];
+    }
+    h[c] = (hv[c] + drp_v(y + 3, a.jdir) + drp_v(z + 3, a.kdir)) * rr;
+    o[c] = (VX + c) * sc + q;
+  }
+  rk_put_n<3>(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, o, h);
+}
+
+// ---------------------------------------------------------------------------
+// stress RHS and RK update at the six volume points i0-3..i0+3 (not i0) of
+// split nodes, one thread per point, x offset fastest
+// (sv_curv_col_el_iso_rhs_fault_stress_F_gpu :432-1159 / _B_gpu :1162-1879,
+// volume points)
+__global__ void __launch_bounds__(192) k_fault_sslab(const FaultArgs a) {
+  const Grid &g = a.g;
+  int j, k, s;
+  if (!slab_item(a, (long)blockIdx.x * blockDim.x + threadIdx.x, j, k, s)) return;
+  const int J = j + NG, K = k + NG;
+  const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny, sc = g.scmp;
+  const FaultDev &F = a.F;
+  if (!(F.flag[nd] & FL_SPLIT)) return;
+  const int i0 = F.i0;
+  const float *w = a.wcur, *met = a.met;
+  const long sy = g.sy, sz = g.sz;
+  const int km = g.nk - (k + 1);
+  const bool fwd = a.idir == 1;
+  const bool top = a.isfree && km == 0;
+  // fault velocity of this side, input level
+  float fV[3];
+  const int m = s < 0 ? 0 : 1;
+#pragma unroll
+  for (int c = 0; c < 3; c++) fV[c] = a.fc[fidx(FVX + c, m, ns, nd)];
+  const long q = g.at(i0 + s, J, K);
+  float dx[3], dy[3], dz[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float *v = w + (VX + c) * sc + q;
+    const float f = fV[c];
+    if (fwd) {
+      // forward operators; points left of the fault see the minus side
+      if (s == 3) dx[c] = drp<1>(v, 1);
+      else if (s == 2) dx[c] = mac24(v, 1, 1);
+      else if (s == 1) dx[c] = mac22(v, 1, 1);
+      else if (s == -1) dx[c] = f - __ldg(v);
+      else if (s == -2) dx[c] = kB1 * __ldg(v) + kB2 * __ldg(v + 1) + kB3 * f;
+      else dx[c] = kC1 * __ldg(v - 1) + kC2 * __ldg(v) + kC3 * __ldg(v + 1) + kC4 * __ldg(v + 2) + kC5 * f;
+    } else {
+      if (s == -3) dx[c] = drp<0>(v, 1);
+      else if (s == -2) dx[c] = mac24(v, 1, 0);
+      else if (s == -1) dx[c] = mac22(v, 1, 0);
+      else if (s == 1) dx[c] = __ldg(v) - f;
+      else if (s == 2) dx[c] = -(kB3 * f + kB2 * __ldg(v - 1) + kB1 * __ldg(v));
+      else dx[c] = -(kC5 * f + kC4 * __ldg(v - 2) + kC3 * __ldg(v - 1) + kC2 * __ldg(v) + kC1 * __ldg(v + 1));
+    }
+    dy[c] = drp_rt(v, sy, a.jdir);
+    if (a.isfree && km == 1) dz[c] = mac22(v, sz, a.kdir);
+    else if (a.isfree && km == 2) dz[c] = mac24(v, sz, a.kdir);
+    else dz[c] = drp_rt(v, sz, a.kdir);
+  }
+  if (top) {
+    const float *X = a.free_mat + ((long)J * g.nx + (i0 + s)) * 9;
+    const float *Y = X + (long)g.ny * g.nx * 9;
+    float o1[3], o2[3];
+    mv3(X, dx, o1); mv3(Y, dy, o2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) dz[c] = o1[c] + o2[c];
+  }
+  float e[3][3];
+#pragma unroll
+  for (int r = 0; r < 9; r++) e[r / 3][r % 3] = __ldg(met + (1 + r) * sc + q);
+  const float lam = __ldg(a.med + q), mu = __ldg(a.med + sc + q);
+  const float l2m = lam + 2.0f * mu;
+  float G[3][3];
+#pragma unroll
+  for (int b = 0; b < 3; b++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) G[c][b] = e[0][b] * dx[c] + e[1][b] * dy[c] + e[2][b] * dz[c];
+  float h[6];
+  h[0] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]);
+  h[1] = l2m * G[1][1] + lam * (G[0][0] + G[2][2]);
+  h[2] = l2m * G[2][2] + lam * (G[0][0] + G[1][1]);
+  h[3] = mu * (G[1][2] + G[2][1]);   // Tyz
+  h[4] = mu * (G[0][2] + G[2][0]);   // Txz
+  h[5] = mu * (G[0][1] + G[1][0]);   // Txy
+  long o[6];
+#pragma unroll
+  for (int c = 0; c < 6; c++) o[c] = (TXX + c) * sc + q;
+  rk_put_n<6>(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, o, h);
+}
+
+// ---------------------------------------------------------------------------
+// split nodes, one thread per node: velocity gradients of both sides
+// (continuity matrices or traction rate, free-surface rows), fault traction
+// rates and their RK update, the split-node volume point of the output
+// level, and after the last stage slip / slip rate / rupture time
+// (sv_curv_col_el_iso_rhs_fault_stress_F_gpu :432-1159 / _B_gpu :1162-1879,
+// split nodes; fault2wave_gpu; fault_var_update_gpu)
+__global__ void __launch_bounds__(128) k_fault_node(const FaultArgs a) {
   const Grid &g = a.g;
   const int j = a.j0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int k = a.k0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -314,11 +516,16 @@ __global__ void __launch_bounds__(128) k_fault_stress(const FaultArgs a) {
   if (!(fl & FL_SPLIT)) return;
   const int i0 = F.i0;
   const float *w = a.wcur, *met = a.met;
-  const long ny = g.ny, sy = g.sy, sz = g.sz;
+  const long ny = g.ny;
   const int km = g.nk - (k + 1);
   const bool fwd = a.idir == 1;
+  const bool top = a.isfree && km == 0;
+  // fault velocity of each side, input level: fV[m][c]
+  float fV[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) { fV[0][c] = a.fc[fidx(FVX + c, 0, ns, nd)]; fV[1][c] = a.fc[fidx(FVX + c, 1, ns, nd)]; }
 
-  // split nodes: along-fault velocity derivatives of each side
+  // along-fault velocity derivatives of each side
   float Sx[2][3], Sy[2][3], Sz[2][3];
 #pragma unroll
   for (int m = 0; m < 2; m++) {
@@ -331,15 +538,8 @@ __global__ void __launch_bounds__(128) k_fault_stress(const FaultArgs a) {
       else Sz[m][c] = (fl & FL_RUPZ) ? mac22(v, ny, a.kdir) : drp_rt(v, ny, a.kdir);
     }
   }
-  const float *fv[3] = { a.fc + fidx(FVX, 0, ns, nd), a.fc + fidx(FVY, 0, ns, nd), a.fc + fidx(FVZ, 0, ns, nd) };
-  // velocity on each side of the fault from the volume: fV[m][c]
-  float fV[2][3];
-#pragma unroll
-  for (int c = 0; c < 3; c++) { fV[0][c] = fv[c][0]; fV[1][c] = fv[c][ns]; }
-
   const float *mat = F.mat;
   auto M = [&](int id) { return mat + ((long)id * ns + nd) * 9; };
-  const bool top = a.isfree && km == 0;
   if (!top) {
     if (a.imethod == 1) {
       // one side from its one-sided difference, the other from continuity
@@ -413,78 +613,21 @@ __global__ void __launch_bounds__(128) k_fault_stress(const FaultArgs a) {
   }
 
   // fault traction rates and RK update of T2, T3 on both sides
+  {
+    long o[12];
+    float h[12];
 #pragma unroll
-  for (int m = 0; m < 2; m++) {
-    const int b2 = m ? FM_D21_2 : FM_D21_1, b3 = m ? FM_D31_2 : FM_D31_1;
-    float g1[3], g2[3], g3[3];
-    mv3(M(b2), Sx[m], g1); mv3(M(b2 + 1), Sy[m], g2); mv3(M(b2 + 2), Sz[m], g3);
+    for (int m = 0; m < 2; m++) {
+      const int b2 = m ? FM_D21_2 : FM_D21_1, b3 = m ? FM_D31_2 : FM_D31_1;
+      float g1[3], g2[3], g3[3];
+      mv3(M(b2), Sx[m], g1); mv3(M(b2 + 1), Sy[m], g2); mv3(M(b2 + 2), Sz[m], g3);
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-      rk_put(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, fidx(FT2X + c, m, ns, nd), g1[c] + g2[c] + g3[c]);
-    mv3(M(b3), Sx[m], g1); mv3(M(b3 + 1), Sy[m], g2); mv3(M(b3 + 2), Sz[m], g3);
+      for (int c = 0; c < 3; c++) { h[6 * m + c] = g1[c] + g2[c] + g3[c]; o[6 * m + c] = fidx(FT2X + c, m, ns, nd); }
+      mv3(M(b3), Sx[m], g1); mv3(M(b3 + 1), Sy[m], g2); mv3(M(b3 + 2), Sz[m], g3);
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-      rk_put(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, fidx(FT3X + c, m, ns, nd), g1[c] + g2[c] + g3[c]);
-  }
-
-  // stress RHS at the six volume points i0+s, s = -3..3 (s != 0)
-#pragma unroll
-  for (int s = -3; s <= 3; s++) {
-    if (s == 0) continue;
-    const long q = g.at(i0 + s, J, K);
-    float dx[3], dy[3], dz[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const float *v = w + (VX + c) * sc + q;
-      const float f = fV[s < 0 ? 0 : 1][c];
-      if (fwd) {
-        // forward operators; points left of the fault see the minus side
-        if (s == 3) dx[c] = drp<1>(v, 1);
-        else if (s == 2) dx[c] = mac24(v, 1, 1);
-        else if (s == 1) dx[c] = mac22(v, 1, 1);
-        else if (s == -1) dx[c] = f - __ldg(v);
-        else if (s == -2) dx[c] = kB1 * __ldg(v) + kB2 * __ldg(v + 1) + kB3 * f;
-        else dx[c] = kC1 * __ldg(v - 1) + kC2 * __ldg(v) + kC3 * __ldg(v + 1) + kC4 * __ldg(v + 2) + kC5 * f;
-      } else {
-        if (s == -3) dx[c] = drp<0>(v, 1);
-        else if (s == -2) dx[c] = mac24(v, 1, 0);
-        else if (s == -1) dx[c] = mac22(v, 1, 0);
-        else if (s == 1) dx[c] = __ldg(v) - f;
-        else if (s == 2) dx[c] = -(kB3 * f + kB2 * __ldg(v - 1) + kB1 * __ldg(v));
-        else dx[c] = -(kC5 * f + kC4 * __ldg(v - 2) + kC3 * __ldg(v - 1) + kC2 * __ldg(v) + kC1 * __ldg(v + 1));
-      }
-      dy[c] = drp_rt(v, sy, a.jdir);
-      if (a.isfree && km == 1) dz[c] = mac22(v, sz, a.kdir);
-      else if (a.isfree && km == 2) dz[c] = mac24(v, sz, a.kdir);
-      else dz[c] = drp_rt(v, sz, a.kdir);
+      for (int c = 0; c < 3; c++) { h[6 * m + 3 + c] = g1[c] + g2[c] + g3[c]; o[6 * m + 3 + c] = fidx(FT3X + c, m, ns, nd); }
     }
-    if (top) {
-      const float *X = a.free_mat + ((long)J * g.nx + (i0 + s)) * 9;
-      const float *Y = X + (long)g.ny * g.nx * 9;
-      float o1[3], o2[3];
-      mv3(X, dx, o1); mv3(Y, dy, o2);
-#pragma unroll
-      for (int c = 0; c < 3; c++) dz[c] = o1[c] + o2[c];
-    }
-    float e[3][3];
-#pragma unroll
-    for (int r = 0; r < 9; r++) e[r / 3][r % 3] = __ldg(met + (1 + r) * sc + q);
-    const float lam = __ldg(a.med + q), mu = __ldg(a.med + sc + q);
-    const float l2m = lam + 2.0f * mu;
-    float G[3][3];
-#pragma unroll
-    for (int b = 0; b < 3; b++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) G[c][b] = e[0][b] * dx[c] + e[1][b] * dy[c] + e[2][b] * dz[c];
-    float h[6];
-    h[0] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]);
-    h[1] = l2m * G[1][1] + lam * (G[0][0] + G[2][2]);
-    h[2] = l2m * G[2][2] + lam * (G[0][0] + G[1][1]);
-    h[3] = mu * (G[1][2] + G[2][1]);   // Tyz
-    h[4] = mu * (G[0][2] + G[2][0]);   // Txz
-    h[5] = mu * (G[0][1] + G[1][0]);   // Txy
-#pragma unroll
-    for (int c = 0; c < 6; c++) rk_put(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, (TXX + c) * sc + q, h[c]);
+    rk_put_n<12>(a.mode, a.ca, a.cb, a.fc, a.fp, a.fo, a.fe, o, h);
   }
 
   // the split-node volume point of the output level from the fault fields
@@ -564,16 +707,28 @@ __global__ void k_advance(Ctl *c, int max_rec) {
 }
 
 // ---------------------------------------------------------------------------
-void launch_fault_stage(const FaultArgs &a, cudaStream_t st) {
+int launch_fault_stage(const FaultArgs &a, cudaStream_t st) {
   {
     dim3 blk(32, 4), grd((a.g.nj + 31) / 32, (a.g.nk + 3) / 4);
     k_fault_weld<<<grd, blk, 0, st>>>(a);
   }
-  if (a.nj > 0 && a.nk > 0) {
-    dim3 blk(32, 4), grd((a.nj + 31) / 32, (a.nk + 3) / 4);
-    k_fault_vel<<<grd, blk, 0, st>>>(a);
-    k_fault_stress<<<grd, blk, 0, st>>>(a);
+  if (a.nj <= 0 || a.nk <= 0) return 1;
+  {
+    const long n = (long)a.tnj * a.tnk * 12;
+    k_fault_trac<<<(unsigned)((n + 191) / 192), 192, 0, st>>>(a);
   }
+  {
+    dim3 blk(32, 4), grd((a.nj + 31) / 32, (a.nk + 3) / 4);
+    k_fault_trial<<<grd, blk, 0, st>>>(a);
+  }
+  const long nslab = (long)a.nj * a.nk * 6;
+  k_fault_vslab<<<(unsigned)((nslab + 191) / 192), 192, 0, st>>>(a);
+  k_fault_sslab<<<(unsigned)((nslab + 191) / 192), 192, 0, st>>>(a);
+  {
+    dim3 blk(32, 4), grd((a.nj + 31) / 32, (a.nk + 3) / 4);
+    k_fault_node<<<grd, blk, 0, st>>>(a);
+  }
+  return 6;
 }
 
 void launch_record(const StationArgs &a, cudaStream_t st) {

@@ -101,6 +101,12 @@ struct FaultArgs {
   int isfree, imethod;
   int j0, k0, nj, nk;          // launch box of split nodes (interior indices)
   Ctl *ctl;
+  // tractions J e_a . sigma of the stage input at x = i0-6..i0-1, i0+1..i0+6
+  // over the split box grown by 3 nodes in j and k: [12][9][tnk][tnj],
+  // components T1 (e_xi), T2 (e_eta), T3 (e_zeta); T2 and T3 only for
+  // |x - i0| <= 3.  tj0 / tk0: ghost-inclusive j / k of element (0, 0).
+  float *trac;
+  int tj0, tk0, tnj, tnk;
 };
 
 struct StationArgs {

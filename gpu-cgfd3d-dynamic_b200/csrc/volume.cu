@@ -151,36 +151,56 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
 #pragma unroll
     for (int c = TXX; c <= TXY; c++) { corr[c] += (cB - 1.0f) * q[c]; ar[c] += cD * q[c]; }
   }
+  // auxiliary RK update; level reads first (see rk_update)
+  float av[9], ev[9];
+#pragma unroll
+  for (int c = 0; c < 9; c++) {
+    const long o = c * P.siz + pa;
+    if (MODE == RK_FIRST) av[c] = __ldg(P.acur + o);
+    else {
+      if (MODE == RK_MID) av[c] = __ldg(P.apre + o);
+      ev[c] = P.aend[o];
+    }
+  }
 #pragma unroll
   for (int c = 0; c < 9; c++) {
     const long o = c * P.siz + pa;
     if (MODE == RK_FIRST) {
-      const float av = __ldg(P.acur + o);
-      P.aout[o] = av + a.ca * ar[c];
-      P.aend[o] = av + a.cb * ar[c];
+      P.aout[o] = av[c] + a.ca * ar[c];
+      P.aend[o] = av[c] + a.cb * ar[c];
     } else if (MODE == RK_MID) {
-      P.aout[o] = __ldg(P.apre + o) + a.ca * ar[c];
-      P.aend[o] += a.cb * ar[c];
+      P.aout[o] = av[c] + a.ca * ar[c];
+      P.aend[o] = ev[c] + a.cb * ar[c];
     } else {
-      P.aend[o] += a.cb * ar[c];
+      P.aend[o] = ev[c] + a.cb * ar[c];
     }
   }
 }
 
+// RK stage update of the nine components at p.  All reads of the levels
+// are issued before the first store: the compiler cannot prove that out
+// and end do not alias, and interleaved load / store pairs would cost one
+// memory round trip per component.
 template <int MODE>
 __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float v0[9], const float h[9]) {
   const long sc = a.g.scmp;
+  if (MODE == RK_FIRST) {
 #pragma unroll
-  for (int c = 0; c < 9; c++) {
-    const long o = c * sc + p;
-    if (MODE == RK_FIRST) {
-      a.out[o] = v0[c] + a.ca * h[c];
-      a.end[o] = v0[c] + a.cb * h[c];
-    } else if (MODE == RK_MID) {
-      a.out[o] = __ldg(a.pre + o) + a.ca * h[c];
-      a.end[o] += a.cb * h[c];
-    } else {
-      a.end[o] += a.cb * h[c];
+    for (int c = 0; c < 9; c++) {
+      a.out[c * sc + p] = v0[c] + a.ca * h[c];
+      a.end[c * sc + p] = v0[c] + a.cb * h[c];
+    }
+  } else {
+    float pv[9], ev[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+      if (MODE == RK_MID) pv[c] = __ldg(a.pre + c * sc + p);
+      ev[c] = a.end[c * sc + p];
+    }
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+      if (MODE == RK_MID) a.out[c * sc + p] = pv[c] + a.ca * h[c];
+      a.end[c * sc + p] = ev[c] + a.cb * h[c];
     }
   }
 }
@@ -213,7 +233,7 @@ __device__ __forceinline__ bool locate(const VolArgs &a, int &i, int &j, int &k)
 }
 
 template <int ID, int JD, int KD, int MODE, int KIND>
-__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 3 : 2) k_volume(const __grid_constant__ VolArgs a) {
+__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 4 : 3) k_volume(const __grid_constant__ VolArgs a) {
   const Grid &g = a.g;
   int i, j, k;
   if (!locate(a, i, j, k)) return;

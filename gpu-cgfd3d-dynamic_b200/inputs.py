@@ -161,7 +161,7 @@ def hills_layered(ni=300, nj=600, nk=240, h=100.0, pml=20, seed=1001, nsta=32,
     st = _stress(nj, nk, fault_grid, (jc - 1, kc), 7)
     sta = np.stack([rng.integers(pml + 4, ni - pml - 4, nsta), rng.integers(pml + 4, nj - pml - 4, nsta),
                     np.full(nsta, nk - 1)], 1).astype(np.float32)
-    fsta = np.array([[jc - 1, kc], [jc - 1 + 100, kc], [jc - 1, nk - 1]], np.float32)
+    fsta = np.array([[jc - 1, kc], [jc - 1 + fault_len // 4, kc], [jc - 1, nk - 1]], np.float32)
     P = ((pml, pml), (pml, pml), (pml, 0))
     vref = ((vp_max, vp_max),) * 3
     return Problem(ni=ni, nj=nj, nk=nk, dt=dt, lam=lam, mu=mu, rho=rho.astype(np.float32),

@@ -6,7 +6,9 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "gpu-cgfd3d-dynamic_b200")
 ORACLE = os.path.join(ROOT, "oracle")
-for p in (PKG, ORACLE):
+TESTS = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(TESTS, "golden")
+for p in (PKG, ORACLE, TESTS, GOLDEN):
     if p not in sys.path:
         sys.path.insert(0, p)
 

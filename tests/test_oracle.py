@@ -1,0 +1,155 @@
+"""CPU tests of the oracle: known answers of the scheme and the golden fixtures.
+
+The reference ships no tests, fixtures or CPU code for this path, so these
+known-answer tests (exact metric of a uniform grid, exact Hooke update of a
+linear velocity field, the CFL bound of a uniform grid, a fault below its
+strength that never moves, a locked fault that converges to the welded
+solution) are what pin the oracle's arithmetic.  The golden fixtures come
+from the double-precision oracle (tests/golden/make_golden.py); the float32
+oracle must reproduce them to rounding.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import inputs
+
+from conftest import GOLDEN
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(np.asarray(b, np.float64)), 1e-30))
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_golden_float_oracle(oracle_built, method):
+    """float32 oracle vs the double-precision fixture (30 steps, 36x56x32)."""
+    import make_golden
+    from oracle import OracleSolver
+    g = np.load(os.path.join(GOLDEN, f"small_planar_m{method}_{make_golden.NSTEPS}.npz"))
+    p = inputs.small_planar(dynamic_method=method, nt=make_golden.NSTEPS)
+    o = OracleSolver(p)
+    o.run(make_golden.NSTEPS)
+    snap = make_golden.snapshot(o, p)
+    assert set(snap) == set(g.files)
+    for k in g.files:
+        assert snap[k].shape == g[k].shape, k
+        assert _rel(snap[k], g[k]) < 1e-4, (k, _rel(snap[k], g[k]))
+    # the run ruptured: slip, a rupture front and peak slip rate above 1 m/s
+    assert g["fault_Slip"].max() > 0.05
+    assert g["fault_Peak_vs"].max() > 1.0
+    assert (g["fault_Init_t0"] > 0).sum() > 100
+
+
+def test_uniform_grid_metric(oracle_built):
+    """Planar fault extrusion at h = 200 m: jac = h^3, xi_x = eta_y = zeta_z = 1/h."""
+    from oracle import OracleSolver
+    p = inputs.small_planar()
+    o = OracleSolver(p)
+    h = 200.0
+    want = {0: h ** 3, 1: 1 / h, 5: 1 / h, 9: 1 / h}
+    for cmp in range(10):
+        m = o.metric(cmp)
+        if cmp in want:
+            np.testing.assert_allclose(m, want[cmp], rtol=1e-5)
+        else:
+            assert np.abs(m).max() < 1e-9, cmp
+
+
+def test_uniform_grid_dt_max(oracle_built):
+    """CFL bound of a uniform grid: 1.3 h / (sqrt(3) Vp) (the point-to-plane
+    distance of calc_dtmax is h / sqrt(3))."""
+    from oracle import OracleSolver
+    p = cases.uniform_box(ni=16, nj=16, nk=16)
+    o = OracleSolver(p)
+    vp = math.sqrt((float(p.lam[0, 0, 0]) + 2 * float(p.mu[0, 0, 0])) / float(p.rho[0, 0, 0]))
+    assert o.dt_max() == pytest.approx(1.3 * 100.0 / (math.sqrt(3.0) * vp), rel=1e-5)
+
+
+def _linear_fields(p, h=100.0):
+    k, j, i = np.meshgrid(np.arange(p.nk), np.arange(p.nj), np.arange(p.ni), indexing="ij")
+    x, y, z = (i - p.ni // 2) * h, (j - p.nj // 2) * h, (k - p.nk + 1) * h
+    G = np.array([[1e-3, 0.0, 2e-3], [1e-3, -5e-4, 0.0], [0.0, -3e-4, 7e-4]])   # G[c][b] = dV_c/dx_b
+    V = {"Vx": G[0, 0] * x + G[0, 2] * z, "Vy": G[1, 0] * x + G[1, 1] * y, "Vz": G[2, 1] * y + G[2, 2] * z}
+    return {c: v.astype(np.float32) for c, v in V.items()}, G
+
+
+def hooke_after_one_step(p, G):
+    lam, mu = float(p.lam[0, 0, 0]), float(p.mu[0, 0, 0])
+    tr = G[0, 0] + G[1, 1] + G[2, 2]
+    T = {"Txx": lam * tr + 2 * mu * G[0, 0], "Tyy": lam * tr + 2 * mu * G[1, 1], "Tzz": lam * tr + 2 * mu * G[2, 2],
+         "Tyz": mu * (G[1, 2] + G[2, 1]), "Txz": mu * (G[0, 2] + G[2, 0]), "Txy": mu * (G[0, 1] + G[1, 0])}
+    return {c: v * p.dt for c, v in T.items()}
+
+
+def check_linear_step(solver, p, V, G):
+    """Away from the boundaries (12 points per step for the 4 stages' 3-point
+    reach), a linear velocity field is a steady state of the momentum
+    equation and one RK4 step sets sigma = dt C grad V exactly: the DRP
+    operators differentiate linear functions exactly."""
+    sl = (slice(14, p.nk - 14), slice(14, p.nj - 14), slice(14, p.ni - 14))
+    want = hooke_after_one_step(p, G)
+    scale = max(abs(v) for v in want.values())
+    for c, v in want.items():
+        got = solver.wavefield(c)[sl]
+        assert np.abs(got - v).max() < 2e-5 * scale, (c, v, got.min(), got.max())
+    for c, v in V.items():
+        assert np.abs(solver.wavefield(c)[sl] - v[sl]).max() < 1e-6 * np.abs(v).max(), c
+
+
+def test_linear_velocity_one_step(oracle_built):
+    from oracle import OracleSolver
+    p = cases.uniform_box(ni=40, nj=40, nk=40, nt=2)
+    V, G = _linear_fields(p)
+    o = OracleSolver(p)
+    for c, v in V.items():
+        o.set_wavefield(c, v)
+    o.run(1)
+    check_linear_step(o, p, V, G)
+
+
+def test_fault_below_strength_stays_locked(oracle_built):
+    """Shear load 60 MPa under a strength of 0.65 x 100 MPa and no
+    nucleation patch: the trial traction never reaches the friction law's
+    bound, the fault never slips and the wavefield stays exactly zero."""
+    from oracle import OracleSolver
+    p = inputs.small_planar(nt=20)
+    p.T0y[0][:] = 60.0e6
+    o = OracleSolver(p)
+    o.run(20)
+    assert o.fault("Vs").max() <= 1e-12
+    assert o.fault("Slip").max() == 0.0
+    assert (o.fault("Init_t0") < 0).all()
+    for c in ("Vx", "Vy", "Vz", "Txx", "Txy"):
+        assert np.abs(o.wavefield(c)).max() == 0.0, c
+    # the traction output stays the initial traction: Tn = -100 MPa, Ts1 = 60 MPa
+    np.testing.assert_allclose(o.fault("Tn"), -100.0e6, rtol=1e-6)
+    np.testing.assert_allclose(o.fault("Ts1"), 60.0e6, rtol=1e-6)
+
+
+def test_locked_fault_matches_welded(oracle_built):
+    """A velocity pulse crossing a fault that cannot slip (mu_s = 1000): the
+    split-node solution keeps the velocity jump at zero and stays within a
+    few percent of the same box without a fault (the difference is the
+    lower-order one-sided operators next to the fault, and shrinks as the
+    pulse widens)."""
+    from oracle import OracleSolver
+    res = {}
+    for fault in (False, True):
+        p = cases.uniform_box(fault=fault, ni=64, nj=48, nk=48, margin=4, nt=100)
+        o = OracleSolver(p)
+        g = cases.gaussian(p, (p.ni // 2 - 16, p.nj // 2, p.nk // 2), 500.0)
+        o.set_wavefield("Vx", g)
+        o.set_wavefield("Vy", 0.5 * g)
+        o.run(90)
+        res[fault] = {c: o.wavefield(c) for c in ("Vx", "Vy", "Txy")}
+        if fault:
+            vs = o.fault("Vs").max()
+    # the pulse reached the fault
+    assert np.abs(res[True]["Vx"][:, :, 32 + 4:]).max() > 0.02
+    assert vs < 1e-6
+    for c in res[False]:
+        assert _rel(res[True][c], res[False][c]) < 0.03, c
