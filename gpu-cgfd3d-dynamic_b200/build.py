@@ -16,7 +16,10 @@ LIB = os.path.join(LIBDIR, "libcgfd.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 
-CU = ["volume.cu", "volume_zq.cu", "volume_tiled.cu", "volume_tma.cu", "fault.cu", "api.cu"]
+# (source, object, extra flags): the volume kernels build as one unit per
+# kernel kind so that they compile in parallel
+CU = [("volume.cu", f"volume_k{k}.cu.o", [f"-DCGFD_VOLUME_KIND={k}"]) for k in range(5)] + [
+    (f, f + ".o", []) for f in ("volume_zq.cu", "volume_tma.cu", "fault.cu", "api.cu")]
 CPP = ["setup.cpp"]
 HEADERS = ["common.h", "ops.cuh", "setup.h"]
 
@@ -41,17 +44,28 @@ def build(verbose=False, ptxas_info=False):
                 print(" ".join(cmd))
             subprocess.check_call(cmd)
         objs.append(obj)
-    for f in CU:
-        src, obj = os.path.join(CSRC, f), os.path.join(BUILD, f + ".o")
+    jobs = []
+    for f, o, extra in CU:
+        src, obj = os.path.join(CSRC, f), os.path.join(BUILD, o)
         if _newer(obj, [src] + hdrs) or ptxas_info:
             cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                                   "--expt-relaxed-constexpr", "-c", src, "-o", obj]
+                                   "--expt-relaxed-constexpr"] + extra + ["-c", src, "-o", obj]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
-            if verbose:
-                print(" ".join(cmd))
-            subprocess.check_call(cmd)
+            jobs.append(cmd)
         objs.append(obj)
+    if jobs:
+        from concurrent.futures import ThreadPoolExecutor
+        if verbose:
+            for cmd in jobs:
+                print(" ".join(cmd))
+        with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+            results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), jobs))
+        for cmd, r in zip(jobs, results):
+            if r.stdout or r.stderr:
+                sys.stderr.write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, cmd)
     if _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp"]
         if verbose:

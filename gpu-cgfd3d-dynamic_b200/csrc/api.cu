@@ -21,10 +21,13 @@
 #include "setup.h"
 
 namespace cgfd {
-void launch_volume(const VolArgs &interior, const VolArgs &shell, int idir, int jdir, int kdir, int mode,
-                   cudaStream_t st);
-void volume_boxes(VolArgs &a, const int (*boxes)[6], int n);
-void launch_volume_tiled(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, int bz);
+int volume_interior_bz();
+void launch_volume_interior(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume_shell(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume_face_x(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void volume_zq_layout(VolArgs &a, const int box[6], int kchunk);
 void launch_volume_zq(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void volume_tma_prepare();
@@ -89,13 +92,17 @@ struct cgfd_solver {
   long long vol_launches = 0;
   int it = 0;
   long long launches_per_step = 0, last_launches = 0;
-  int tiled = 0, kchunk = 32;           // volume kernel: 0 boxes, 1 smem-tiled, 2 TMA-fed, 3 z-marching interior + boxes
+  int tiled = 0, kchunk = 32;           // volume kernels: 0 boxes, 2 TMA-fed, 3 z-marching interior + boxes
   int kchunk_zq = 32;
   int kchunk_tma = 32;
   int box_top[1][6];                    // rows under the free surface
   CUtensorMap tmap[4];                  // TMA maps of the 4 level slots
   int box_in[1][6];                     // interior box (no PML, no surface rows)
-  int box_shell[6][6];                  // PML slabs and surface rows
+  // boxes of each volume kernel kind: 0 interior, 1 generic shell (PML
+  // edges / corners, surface rows), 2..4 slabs reached by the PML faces of
+  // one direction only (x, y, z)
+  int kbox[5][12][6];
+  int nkbox[5] = {};
   std::vector<void *> allocs;
 };
 
@@ -174,7 +181,7 @@ void enqueue_step(cgfd_solver *s, int it) {
     // external event nodes when captured, so that the events really fire
     // on every graph replay
     if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
-    VolArgs vi = v, vs = v;
+    VolArgs vs = v;
     v.kchunk = s->kchunk;
     v.ctl_err = &s->ctl->err;
     if (s->tiled == 2) {
@@ -183,30 +190,33 @@ void enqueue_step(cgfd_solver *s, int it) {
       v.kend = s->isfree ? s->g.nk - 4 : s->g.nk;
       v.kchunk = s->kchunk_tma;
       launch_volume_tma(s->tmap[scur], v, idir, jdir, kdir, mode, s->stream);
-      vi.nbox = 0;
-      volume_boxes(vs, s->box_top, 1);
-      VolArgs none = vs;
-      none.nbox = 0;
-      launch_volume(none, vs, idir, jdir, kdir, mode, s->stream);
+      volume_boxes(vs, s->box_top, 1, 1);
+      launch_volume_shell(vs, idir, jdir, kdir, mode, s->stream);
       nl += 1 + (vs.nbox > 0);
-    } else if (s->tiled == 1) {
-      launch_volume_tiled(v, idir, jdir, kdir, mode, s->stream);
-      nl += 1;
-    } else if (s->tiled == 3) {
-      // interior box: z-marching kernel; PML slabs and surface rows: boxes
-      VolArgs vz = v;
-      volume_zq_layout(vz, s->box_in[0], s->kchunk_zq);
-      launch_volume_zq(vz, idir, jdir, kdir, mode, s->stream);
-      volume_boxes(vs, s->box_shell, 6);
-      VolArgs none = vs;
-      none.nbox = 0;
-      launch_volume(none, vs, idir, jdir, kdir, mode, s->stream);
-      nl += (vz.nbox > 0) + (vs.nbox > 0);
     } else {
-      volume_boxes(vi, s->box_in, 1);
-      volume_boxes(vs, s->box_shell, 6);
-      launch_volume(vi, vs, idir, jdir, kdir, mode, s->stream);
-      nl += (vi.nbox > 0) + (vs.nbox > 0);
+      // interior box (z-marching kernel when selected), single-direction
+      // PML slabs, generic shell
+      int kind0 = 0;
+      if (s->tiled == 3) {
+        VolArgs vz = v;
+        volume_zq_layout(vz, s->box_in[0], s->kchunk_zq);
+        launch_volume_zq(vz, idir, jdir, kdir, mode, s->stream);
+        nl += vz.nbox > 0;
+        kind0 = 1;
+      }
+      for (int kind = kind0; kind < 5; kind++) {
+        VolArgs vk = vs;
+        volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind == 0 ? volume_interior_bz() : 1);
+        if (vk.nbox == 0) continue;
+        switch (kind) {
+          case 0: launch_volume_interior(vk, idir, jdir, kdir, mode, s->stream); break;
+          case 1: launch_volume_shell(vk, idir, jdir, kdir, mode, s->stream); break;
+          case 2: launch_volume_face_x(vk, idir, jdir, kdir, mode, s->stream); break;
+          case 3: launch_volume_face_y(vk, idir, jdir, kdir, mode, s->stream); break;
+          default: launch_volume_face_z(vk, idir, jdir, kdir, mode, s->stream); break;
+        }
+        nl += vk.nbox > 0;
+      }
     }
     if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
   }
@@ -304,7 +314,6 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   const char *vk = std::getenv("CGFD_VOLUME");
   s->tiled = 0;
   if (vk && std::strcmp(vk, "tma") == 0) s->tiled = 2;
-  if (vk && std::strcmp(vk, "tiled") == 0) s->tiled = 1;
   if (vk && std::strcmp(vk, "zq") == 0) s->tiled = 3;
   {
     // z chunk per block: enough blocks for several waves, rows >= 8
@@ -402,14 +411,37 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     const int klo = L(2, 0), khi = s->isfree ? g.nk - 5 : g.nk - 1 - L(2, 1);
     const int bi[6] = { ilo, ihi, jlo, jhi, klo, khi };
     std::memcpy(s->box_in[0], bi, sizeof bi);
-    const int sh[6][6] = {
-      { 0, ilo - 1, 0, g.nj - 1, 0, g.nk - 1 },
-      { ihi + 1, g.ni - 1, 0, g.nj - 1, 0, g.nk - 1 },
-      { ilo, ihi, 0, jlo - 1, 0, g.nk - 1 },
-      { ilo, ihi, jhi + 1, g.nj - 1, 0, g.nk - 1 },
-      { ilo, ihi, jlo, jhi, 0, klo - 1 },
-      { ilo, ihi, jlo, jhi, khi + 1, g.nk - 1 } };
-    std::memcpy(s->box_shell, sh, sizeof sh);
+    auto add = [&](int kind, int i0, int i1, int j0, int j1, int k0, int k1) {
+      if (i1 < i0 || j1 < j0 || k1 < k0) return;
+      int *b = s->kbox[kind][s->nkbox[kind]++];
+      b[0] = i0; b[1] = i1; b[2] = j0; b[3] = j1; b[4] = k0; b[5] = k1;
+    };
+    const int ni = g.ni, nj = g.nj, nk = g.nk;
+    add(0, ilo, ihi, jlo, jhi, klo, khi);
+    // one PML direction only
+    add(2, 0, ilo - 1, jlo, jhi, klo, khi);
+    add(2, ihi + 1, ni - 1, jlo, jhi, klo, khi);
+    add(3, ilo, ihi, 0, jlo - 1, klo, khi);
+    add(3, ilo, ihi, jhi + 1, nj - 1, klo, khi);
+    add(4, ilo, ihi, jlo, jhi, 0, klo - 1);
+    if (!s->isfree) add(4, ilo, ihi, jlo, jhi, khi + 1, nk - 1);
+    // vertical edges, bottom ring, top ring or surface rows
+    add(1, 0, ilo - 1, 0, jlo - 1, klo, khi);
+    add(1, 0, ilo - 1, jhi + 1, nj - 1, klo, khi);
+    add(1, ihi + 1, ni - 1, 0, jlo - 1, klo, khi);
+    add(1, ihi + 1, ni - 1, jhi + 1, nj - 1, klo, khi);
+    add(1, 0, ilo - 1, 0, nj - 1, 0, klo - 1);
+    add(1, ihi + 1, ni - 1, 0, nj - 1, 0, klo - 1);
+    add(1, ilo, ihi, 0, jlo - 1, 0, klo - 1);
+    add(1, ilo, ihi, jhi + 1, nj - 1, 0, klo - 1);
+    if (s->isfree) {
+      add(1, 0, ni - 1, 0, nj - 1, khi + 1, nk - 1);
+    } else {
+      add(1, 0, ilo - 1, 0, nj - 1, khi + 1, nk - 1);
+      add(1, ihi + 1, ni - 1, 0, nj - 1, khi + 1, nk - 1);
+      add(1, ilo, ihi, 0, jlo - 1, khi + 1, nk - 1);
+      add(1, ilo, ihi, jhi + 1, nj - 1, khi + 1, nk - 1);
+    }
     const int bt[6] = { 0, g.ni - 1, 0, g.nj - 1, s->isfree ? g.nk - 4 : g.nk, g.nk - 1 };
     std::memcpy(s->box_top[0], bt, sizeof bt);
     // z chunk of the z-marching kernel: about 8 waves of 2 blocks per SM

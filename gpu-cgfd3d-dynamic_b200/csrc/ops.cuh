@@ -63,7 +63,7 @@ enum { RK_FIRST = 0, RK_MID = 1, RK_LAST = 2 };
 // a box of interior points (inclusive bounds) covered by one launch;
 // blocks [first, next box's first) belong to it
 struct VolBox {
-  int i0, i1, j0, j1, k0;
+  int i0, i1, j0, j1, k0, k1;
   int nbx, nby, first;
 };
 
@@ -73,7 +73,7 @@ struct VolArgs {
   int kend;                    // rows [0, kend) handled by the TMA kernel
   int *ctl_err;                // Ctl::err of the solver
   int nbox, nblocks;
-  VolBox box[7];
+  VolBox box[12];
   const float *cur, *pre;
   float *out, *end;            // next-stage level (null at the last stage), E
   const float *met, *med, *free_mat;

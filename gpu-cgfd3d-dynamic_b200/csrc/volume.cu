@@ -37,6 +37,12 @@ namespace cgfd {
 namespace {
 
 constexpr int BX = 32, BY = 8;
+// z rows per block of the interior kernel (blocks of 32 x 8/IBZ x IBZ):
+// taps along z of neighbouring rows then meet in L1
+#ifndef CGFD_INTERIOR_BZ
+#define CGFD_INTERIOR_BZ 1
+#endif
+constexpr int IBZ = CGFD_INTERIOR_BZ;
 
 // conservative traction J * (e . sigma_row) at point q for metric row `ax`
 // (MXIX, METX or MZTX) and stress row r (0: xx,xy,xz; 1: xy,yy,yz;
@@ -205,10 +211,15 @@ __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float 
   }
 }
 
-enum { INTERIOR = 0, SHELL = 1 };
+// kernel kinds: the interior box (no boundary logic), slabs that only PML
+// faces of one direction reach (x, y or z), and the generic shell (edges
+// and corners where faces overlap, rows under the free surface)
+enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4 };
 
 // block -> point; boxes with a narrow x extent (PML x slabs) pack their
-// points densely instead of leaving most of a 32-wide row idle
+// points densely instead of leaving most of a 32-wide row idle; blocks of
+// the interior kernel cover BZ z rows (threadIdx.z)
+template <int BZ>
 __device__ __forceinline__ bool locate(const VolArgs &a, int &i, int &j, int &k) {
   int b = 0;
 #pragma unroll 1
@@ -227,16 +238,17 @@ __device__ __forceinline__ bool locate(const VolArgs &a, int &i, int &j, int &k)
   }
   const int bx = bid % B.nbx, rem = bid / B.nbx, by = rem % B.nby, bz = rem / B.nby;
   i = B.i0 + bx * BX + threadIdx.x;
-  j = B.j0 + by * BY + threadIdx.y;
-  k = B.k0 + bz;
-  return i <= B.i1 && j <= B.j1;
+  j = B.j0 + by * (BY / BZ) + threadIdx.y;
+  k = B.k0 + bz * BZ + threadIdx.z;
+  return i <= B.i1 && j <= B.j1 && k <= B.k1;
 }
 
 template <int ID, int JD, int KD, int MODE, int KIND>
 __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 4 : 3) k_volume(const __grid_constant__ VolArgs a) {
+  static_assert(KIND >= INTERIOR && KIND <= FACE_Z, "kernel kind");
   const Grid &g = a.g;
   int i, j, k;
-  if (!locate(a, i, j, k)) return;
+  if (!locate<KIND == INTERIOR ? IBZ : 1>(a, i, j, k)) return;
   const int I = i + NG, J = j + NG, K = k + NG;
   // split-node slabs (i0-3..i0+3 of unwelded nodes) belong to the fault kernels
   for (int f = 0; f < a.nfault; f++) {
@@ -277,7 +289,38 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 4 : 3) k_volume(co
     return;
   }
 
-  // ---- shell: PML slabs and the rows under the free surface ----------------
+  if (KIND >= FACE_X) {
+    // one PML direction FD: the other two directions accumulate like the
+    // interior, direction FD is kept apart for the face's correction and
+    // auxiliary update
+    constexpr int FD = KIND - FACE_X;
+    constexpr int FF = FD == 0 ? ID : (FD == 1 ? JD : KD);
+    float G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
+    float s[3] = { 0.f, 0.f, 0.f };
+    if (FD != 0) acc_dir<ID>(w, sc, v0, ox, e[0], G, s);
+    if (FD != 1) acc_dir<JD>(w, sc, v0, oy, e[1], G, s);
+    if (FD != 2) acc_dir<KD>(w, sc, v0, oz, e[2], G, s);
+    float D[9], r[9], corr[9];
+    derivs<FF>(w, sc, v0, FD == 0 ? ox : (FD == 1 ? oy : oz), D);
+    rhs_dir(D, e[FD], lam, mu, l2m, slw, r);
+    h[VX] = slw * s[0] + r[VX]; h[VY] = slw * s[1] + r[VY]; h[VZ] = slw * s[2] + r[VZ];
+    h[TXX] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]) + r[TXX];
+    h[TYY] = l2m * G[1][1] + lam * (G[0][0] + G[2][2]) + r[TYY];
+    h[TZZ] = l2m * G[2][2] + lam * (G[0][0] + G[1][1]) + r[TZZ];
+    h[TXY] = mu * (G[0][1] + G[1][0]) + r[TXY];
+    h[TXZ] = mu * (G[0][2] + G[2][0]) + r[TXZ];
+    h[TYZ] = mu * (G[1][2] + G[2][1]) + r[TYZ];
+#pragma unroll
+    for (int c = 0; c < 9; c++) corr[c] = 0.f;
+    if (a.pml[2 * FD].on) pml_face<MODE>(a, a.pml[2 * FD], FD, I, J, K, r, D, e[2], lam, mu, l2m, false, 0, corr);
+    if (a.pml[2 * FD + 1].on) pml_face<MODE>(a, a.pml[2 * FD + 1], FD, I, J, K, r, D, e[2], lam, mu, l2m, false, 0, corr);
+#pragma unroll
+    for (int c = 0; c < 9; c++) h[c] += corr[c];
+    rk_update<MODE>(a, p, v0, h);
+    return;
+  }
+
+  // ---- shell: PML edges and corners, rows under the free surface ----------
   const int nk2 = g.nk + NG - 1;
   const bool top = a.isfree && K >= nk2 - 3;
   const bool surfrow = a.isfree && K == nk2;
@@ -367,7 +410,8 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 4 : 3) k_volume(co
 template <int ID, int JD, int KD, int KIND>
 void launch4(const VolArgs &a, int mode, cudaStream_t st) {
   if (a.nbox == 0) return;
-  const dim3 blk(BX, BY, 1);
+  constexpr int BZ = KIND == INTERIOR ? IBZ : 1;
+  const dim3 blk(BX, BY / BZ, BZ);
   const dim3 grd(a.nblocks);
   if (mode == RK_FIRST) k_volume<ID, JD, KD, RK_FIRST, KIND><<<grd, blk, 0, st>>>(a);
   else if (mode == RK_MID) k_volume<ID, JD, KD, RK_MID, KIND><<<grd, blk, 0, st>>>(a);
@@ -390,18 +434,31 @@ void launch_kind(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaS
 
 }  // namespace
 
+// This file is compiled once per kernel kind (CGFD_VOLUME_KIND = 0..4, set
+// by the build) so that the 24 instantiations of each kind build in
+// parallel; unit 0 also holds the host helpers.
+#ifndef CGFD_VOLUME_KIND
+#define CGFD_VOLUME_KIND 0
+#endif
+
+#if CGFD_VOLUME_KIND == 0
 // boxes (interior indices, inclusive) -> block layout of one launch; boxes
 // at most 24 points wide in x are packed (nbx = 0)
-void volume_boxes(VolArgs &a, const int (*boxes)[6], int n) {
+void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, int bz) {
   a.nbox = 0;
   int first = 0;
   for (int q = 0; q < n; q++) {
     const int *b = boxes[q];
     if (b[1] < b[0] || b[3] < b[2] || b[5] < b[4]) continue;
     VolBox &B = a.box[a.nbox++];
-    B.i0 = b[0]; B.i1 = b[1]; B.j0 = b[2]; B.j1 = b[3]; B.k0 = b[4];
+    B.i0 = b[0]; B.i1 = b[1]; B.j0 = b[2]; B.j1 = b[3]; B.k0 = b[4]; B.k1 = b[5];
     const int ni = b[1] - b[0] + 1, nj = b[3] - b[2] + 1, nk = b[5] - b[4] + 1;
-    if (ni <= 24) {
+    if (bz > 1) {
+      B.nbx = (ni + BX - 1) / BX;
+      B.nby = (nj + BY / bz - 1) / (BY / bz);
+      B.first = first;
+      first += B.nbx * B.nby * ((nk + bz - 1) / bz);
+    } else if (ni <= 24) {
       B.nbx = 0;
       B.nby = (ni * nj + BX * BY - 1) / (BX * BY);
       B.first = first;
@@ -416,10 +473,27 @@ void volume_boxes(VolArgs &a, const int (*boxes)[6], int n) {
   a.nblocks = first;
 }
 
-void launch_volume(const VolArgs &interior, const VolArgs &shell, int idir, int jdir, int kdir, int mode,
-                   cudaStream_t st) {
-  launch_kind<INTERIOR>(interior, idir, jdir, kdir, mode, st);
-  launch_kind<SHELL>(shell, idir, jdir, kdir, mode, st);
+int volume_interior_bz() { return IBZ; }
+
+void launch_volume_interior(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<INTERIOR>(a, idir, jdir, kdir, mode, st);
 }
+#elif CGFD_VOLUME_KIND == 1
+void launch_volume_shell(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<SHELL>(a, idir, jdir, kdir, mode, st);
+}
+#elif CGFD_VOLUME_KIND == 2
+void launch_volume_face_x(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<FACE_X>(a, idir, jdir, kdir, mode, st);
+}
+#elif CGFD_VOLUME_KIND == 3
+void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<FACE_Y>(a, idir, jdir, kdir, mode, st);
+}
+#else
+void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<FACE_Z>(a, idir, jdir, kdir, mode, st);
+}
+#endif
 
 }  // namespace cgfd

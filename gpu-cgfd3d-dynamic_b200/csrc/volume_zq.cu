@@ -264,7 +264,7 @@ void volume_zq_layout(VolArgs &a, const int box[6], int kchunk) {
   a.nblocks = 0;
   if (box[1] < box[0] || box[3] < box[2] || box[5] < box[4]) return;
   VolBox &B = a.box[0];
-  B.i0 = box[0]; B.i1 = box[1]; B.j0 = box[2]; B.j1 = box[3]; B.k0 = box[4];
+  B.i0 = box[0]; B.i1 = box[1]; B.j0 = box[2]; B.j1 = box[3]; B.k0 = box[4]; B.k1 = box[5];
   B.nbx = (box[1] - box[0] + ZX) / ZX;
   B.nby = (box[3] - box[2] + ZY) / ZY;
   B.first = 0;
