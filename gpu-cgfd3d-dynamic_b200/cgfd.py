@@ -221,6 +221,8 @@ def load_library(path: str = LIB_PATH):
     lib.cgfd_setup_free.restype = None
     lib.cgfd_set_timing.argtypes = [vp, C.c_int]
     lib.cgfd_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+    lib.cgfd_last_kernel_timing.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                            C.POINTER(C.c_longlong)]
     _lib = lib
     return lib
 
@@ -287,6 +289,13 @@ class Solver:
         a, b, n = C.c_double(), C.c_double(), C.c_longlong()
         self._check(self.lib.cgfd_last_timing(self.h, C.byref(a), C.byref(b), C.byref(n)))
         return a.value, b.value, n.value
+
+    def kernel_timing(self, which):
+        """(ms, launches, points per launch) of the last run() with timing on:
+        which 0 = the whole volume stage, 1 = the interior-box kernel."""
+        a, n, p = C.c_double(), C.c_longlong(), C.c_longlong()
+        self._check(self.lib.cgfd_last_kernel_timing(self.h, int(which), C.byref(a), C.byref(n), C.byref(p)))
+        return a.value, n.value, p.value
 
     def _check(self, rc):
         if rc != 0:

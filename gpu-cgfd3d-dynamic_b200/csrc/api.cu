@@ -88,8 +88,10 @@ struct cgfd_solver {
   int timing = 0;
   cudaEvent_t ev_run[2] = {};
   cudaEvent_t ev_vol[8][4][2] = {};
-  double run_ms = 0, vol_ms = 0;
-  long long vol_launches = 0;
+  cudaEvent_t ev_int[8][4] = {};        // after the interior-box kernel
+  double run_ms = 0, vol_ms = 0, int_ms = 0;
+  long long vol_launches = 0, int_launches = 0;
+  long long int_points = 0, vol_points = 0;   // points one launch updates
   int it = 0;
   long long launches_per_step = 0, last_launches = 0;
   int tiled = 0, kchunk = 32;           // volume kernels: 0 boxes, 2 TMA-fed, 3 z-marching interior + boxes
@@ -132,6 +134,8 @@ void destroy(cgfd_solver *s) {
   for (int q = 0; q < 2; q++) if (s->ev_run[q]) cudaEventDestroy(s->ev_run[q]);
   for (int a = 0; a < 8; a++) for (int b = 0; b < 4; b++) for (int c = 0; c < 2; c++)
     if (s->ev_vol[a][b][c]) cudaEventDestroy(s->ev_vol[a][b][c]);
+  for (int a = 0; a < 8; a++) for (int b = 0; b < 4; b++)
+    if (s->ev_int[a][b]) cudaEventDestroy(s->ev_int[a][b]);
   for (void *p : s->allocs) cudaFree(p);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -209,7 +213,10 @@ void enqueue_step(cgfd_solver *s, int it) {
         volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind == 0 ? volume_interior_bz() : 1);
         if (vk.nbox == 0) continue;
         switch (kind) {
-          case 0: launch_volume_interior(vk, idir, jdir, kdir, mode, s->stream); break;
+          case 0:
+            launch_volume_interior(vk, idir, jdir, kdir, mode, s->stream);
+            if (s->timing) cudaEventRecordWithFlags(s->ev_int[ip][stage], s->stream, cudaEventRecordExternal);
+            break;
           case 1: launch_volume_shell(vk, idir, jdir, kdir, mode, s->stream); break;
           case 2: launch_volume_face_x(vk, idir, jdir, kdir, mode, s->stream); break;
           case 3: launch_volume_face_y(vk, idir, jdir, kdir, mode, s->stream); break;
@@ -455,11 +462,30 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     s->kchunk_zq = (int)std::max<long>(16, (nz + nch - 1) / nch);
     const char *kc = std::getenv("CGFD_ZQ_KCHUNK");
     if (kc && std::atoi(kc) > 0) s->kchunk_zq = std::atoi(kc);
+    // points one interior launch / one volume stage updates: the split-node
+    // slabs belong to the fault kernels
+    long long nint = (long long)std::max(0, ihi - ilo + 1) * std::max(0, jhi - jlo + 1) * std::max(0, khi - klo + 1);
+    long long nall = (long long)ni * nj * nk;
+    for (size_t f = 0; f < H.faults.size(); f++) {
+      const FaultHost &Fh = H.faults[f];
+      for (int k = 0; k < nk; k++) for (int j = 0; j < nj; j++) {
+        if (!(Fh.flag[(size_t)(j + NG) + (size_t)(k + NG) * g.ny] & FL_SPLIT)) continue;
+        for (int d = -3; d <= 3; d++) {
+          const int i = Fh.i0 - NG + d;
+          if (i < 0 || i >= ni) continue;
+          nall--;
+          if (i >= ilo && i <= ihi && j >= jlo && j <= jhi && k >= klo && k <= khi) nint--;
+        }
+      }
+    }
+    s->int_points = nint;
+    s->vol_points = nall;
   }
   CK(dalloc(s, &s->ctl, 1), "control block");
   for (int q = 0; q < 2; q++) CK(cudaEventCreate(&s->ev_run[q]), "event");
   for (int a = 0; a < 8; a++) for (int b = 0; b < 4; b++) for (int c = 0; c < 2; c++)
     CK(cudaEventCreate(&s->ev_vol[a][b][c]), "event");
+  for (int a = 0; a < 8; a++) for (int b = 0; b < 4; b++) CK(cudaEventCreate(&s->ev_int[a][b]), "event");
   CK(cudaStreamSynchronize(s->stream), "set-up");
 #undef CK
   *out = s;
@@ -469,8 +495,9 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
 int cgfd_run(cgfd_solver *s, int nsteps) {
   if (!s || nsteps < 0) return fail(CGFD_ERR_ARG, "bad argument");
   long long nl = 0;
-  double vol_ms = 0;
-  long long vol_n = 0;
+  double vol_ms = 0, int_ms = 0;
+  long long vol_n = 0, int_n = 0;
+  const bool int_timed = s->tiled == 0 && s->nkbox[0] > 0;
   cudaError_t e = cudaEventRecord(s->ev_run[0], s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "event");
   for (int q = 0; q < nsteps; q++) {
@@ -505,6 +532,11 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
         cudaEventElapsedTime(&ms, s->ev_vol[it % 8][st][0], s->ev_vol[it % 8][st][1]);
         vol_ms += ms;
         vol_n++;
+        if (int_timed) {
+          cudaEventElapsedTime(&ms, s->ev_vol[it % 8][st][0], s->ev_int[it % 8][st]);
+          int_ms += ms;
+          int_n++;
+        }
       }
     }
     nl += s->launches_per_step;
@@ -518,6 +550,7 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   float run_ms = 0;
   cudaEventElapsedTime(&run_ms, s->ev_run[0], s->ev_run[1]);
   s->run_ms = run_ms; s->vol_ms = vol_ms; s->vol_launches = vol_n;
+  s->int_ms = int_ms; s->int_launches = int_n;
   Ctl c;
   e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read control block");
@@ -538,6 +571,14 @@ int cgfd_last_timing(const cgfd_solver *s, double *run_ms, double *volume_ms, lo
   if (run_ms) *run_ms = s->run_ms;
   if (volume_ms) *volume_ms = s->vol_ms;
   if (volume_launches) *volume_launches = s->vol_launches;
+  return CGFD_OK;
+}
+
+int cgfd_last_kernel_timing(const cgfd_solver *s, int which, double *ms, long long *launches, long long *points) {
+  if (!s || which < 0 || which > 1) return fail(CGFD_ERR_ARG, "bad argument");
+  if (ms) *ms = which ? s->int_ms : s->vol_ms;
+  if (launches) *launches = which ? s->int_launches : s->vol_launches;
+  if (points) *points = which ? s->int_points : s->vol_points;
   return CGFD_OK;
 }
 

@@ -218,6 +218,13 @@ int cgfd_set_timing(cgfd_solver *s, int on);
  * volume-stage launches. */
 int cgfd_last_timing(const cgfd_solver *s, double *run_ms, double *volume_ms,
                      long long *volume_launches);
+/* Per-kernel detail of the last cgfd_run with timing on (no counterpart in
+ * the reference; instrumentation for roofline figures).  which = 0: the
+ * volume stage (all volume kernels of one RK stage); which = 1: the
+ * interior-box kernel alone.  ms: summed device time of the timed launches;
+ * launches: their number; points: grid points one launch updates. */
+int cgfd_last_kernel_timing(const cgfd_solver *s, int which, double *ms,
+                            long long *launches, long long *points);
 
 /* Release device and host memory of the handle. */
 void cgfd_destroy(cgfd_solver *s);
