@@ -66,33 +66,18 @@ def make_problem(workload):
 
 
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local
+    import replicas
+    return replicas.init("nccl")
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    import replicas
+    replicas.barrier(ws)
 
 
 def allmax(ws, x):
-    if ws <= 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    import replicas
+    return replicas.allmax(ws, x, "cuda")
 
 
 class ClockSampler:
@@ -222,7 +207,8 @@ def main():
     run_ms_max = allmax(ws, run_ms)
     vol_ms_max = allmax(ws, vol_ms)
     int_ms_max = allmax(ws, int_ms)
-    value = prob.points * args.steps * ws / (run_ms_max / 1e3) / 1e9
+    import replicas
+    value = replicas.aggregate_rate(prob.points, args.steps, ws, run_ms_max / 1e3) / 1e9
     peak, peak_kind = peaks()
     # dominant kernel: the interior-box volume kernel; one launch is one RK
     # stage of int_pts points at 768 / 4 = 192 algorithmic bytes each
@@ -277,9 +263,7 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": unit, "cores": th, "kind": "port", "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish(ws)
 
 
 if __name__ == "__main__":

@@ -91,3 +91,24 @@ def test_hills_layered_small(cgfd_lib, oracle_built, method):
     assert rel_l2(s.stations()[:, :3], o.stations()[:, :3]) < 1e-4
     for c in range(9):
         assert rel_l2(s.wavefield(c), o.wavefield(c)) < 1e-4, WAVE_COMPONENTS[c]
+
+
+def test_tpv_planar_full_600_steps(cgfd_lib, oracle_built):
+    """The 160x100x80 planar case in full (h = 200 m, 10-layer PML, flat
+    free surface, 600 steps of 0.01 s): slip rate, slip, peak slip rate and
+    station velocity within relative L2 1e-4 of the oracle, the rupture time
+    of every node within one time step, the same set of ruptured nodes."""
+    from oracle import OracleSolver
+    p = inputs.tpv_planar()
+    s, o = Solver(p), OracleSolver(p)
+    s.run(600)
+    o.run(600)
+    for f in ("Vs", "Slip", "Peak_vs", "Tn", "Ts1"):
+        assert rel_l2(s.fault(f), o.fault(f)) < 1e-4, f
+    t0s, t0o = s.fault("Init_t0"), o.fault("Init_t0")
+    rup = t0o > 0
+    assert rup.sum() > 1000
+    assert np.array_equal(t0s > 0, rup)
+    assert np.abs(t0s[rup] - t0o[rup]).max() <= p.dt * 1.0001
+    assert rel_l2(s.stations()[:, :3], o.stations()[:, :3]) < 1e-4
+    assert rel_l2(s.fault_stations(), o.fault_stations()) < 1e-4
