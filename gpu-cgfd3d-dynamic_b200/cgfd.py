@@ -221,6 +221,7 @@ def load_library(path: str = LIB_PATH):
     lib.cgfd_setup_free.restype = None
     lib.cgfd_set_timing.argtypes = [vp, C.c_int]
     lib.cgfd_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+    lib.cgfd_run_noalloc.argtypes = [vp, C.c_int]
     lib.cgfd_last_kernel_timing.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                             C.POINTER(C.c_longlong)]
     _lib = lib
@@ -289,6 +290,12 @@ class Solver:
         a, b, n = C.c_double(), C.c_double(), C.c_longlong()
         self._check(self.lib.cgfd_last_timing(self.h, C.byref(a), C.byref(b), C.byref(n)))
         return a.value, b.value, n.value
+
+    def run_noalloc(self, nsteps: int):
+        """Advance like run(), allocating nothing (cgfd_run_noalloc): direct
+        launches, traction scratch in the library's fixed device array.  Calls
+        on one device must not overlap."""
+        self._check(self.lib.cgfd_run_noalloc(self.h, int(nsteps)))
 
     def kernel_timing(self, which):
         """(ms, launches, points per launch) of the last run() with timing on:

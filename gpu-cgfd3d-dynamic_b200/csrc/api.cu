@@ -12,6 +12,8 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <atomic>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -35,6 +37,7 @@ int volume_tma_encode(CUtensorMap *tm, const float *level, const Grid &g);
 void launch_volume_tma(const CUtensorMap &tm, const VolArgs &a, int idir, int jdir, int kdir, int mode,
                        cudaStream_t st);
 int launch_fault_stage(const FaultArgs &a, cudaStream_t st);
+cudaError_t noalloc_scratch_address(float **p);
 void launch_record(const StationArgs &a, cudaStream_t st);
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
 }  // namespace cgfd
@@ -44,7 +47,10 @@ using namespace cgfd;
 namespace {
 
 thread_local std::string g_err;
-int fail(int code, const std::string &m) { g_err = m; return code; }
+// messages of cgfd_run_noalloc go to a fixed buffer (no allocation)
+thread_local char g_err_fixed[256];
+thread_local bool g_err_is_fixed = false;
+int fail(int code, const std::string &m) { g_err = m; g_err_is_fixed = false; return code; }
 
 // FD_Flags (src/forward/fd_t.cu:146-159): 0 backward, 1 forward
 const int kPairs[8][3] = { {0,0,0},{1,1,0},{1,1,1},{0,0,1},{0,1,0},{1,0,0},{1,0,1},{0,1,1} };
@@ -141,9 +147,12 @@ void destroy(cgfd_solver *s) {
   delete s;
 }
 
-// enqueue one time step (graph capture or direct launches)
-void enqueue_step(cgfd_solver *s, int it) {
+// enqueue one time step (graph capture or direct launches); trac: traction
+// scratch to use instead of each fault's own (cgfd_run_noalloc); timed:
+// whether the solver's timing events may be recorded
+void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = true) {
   const int ip = it % 8;
+  const bool tm = s->timing && timed;
   long long nl = 0;
   StationArgs sa{};
   sa.g = s->g; sa.st = s->st; sa.w = s->w[slot(LP, it)]; sa.ns = (long)s->g.ny * s->g.nz; sa.ctl = s->ctl;
@@ -167,7 +176,7 @@ void enqueue_step(cgfd_solver *s, int it) {
       a.ca = ca; a.cb = cb; a.rkb = kRkB[stage]; a.dt = s->dt;
       a.isfree = s->isfree; a.imethod = s->imethod;
       a.j0 = F.j0; a.k0 = F.k0; a.nj = F.nj; a.nk = F.nk; a.ctl = s->ctl;
-      a.trac = F.trac; a.tj0 = F.j0 + NG - 3; a.tk0 = F.k0 + NG - 3; a.tnj = F.nj + 6; a.tnk = F.nk + 6;
+      a.trac = trac ? trac : F.trac; a.tj0 = F.j0 + NG - 3; a.tk0 = F.k0 + NG - 3; a.tnj = F.nj + 6; a.tnk = F.nk + 6;
       nl += launch_fault_stage(a, s->stream);
     }
     VolArgs v{};
@@ -184,7 +193,7 @@ void enqueue_step(cgfd_solver *s, int it) {
     }
     // external event nodes when captured, so that the events really fire
     // on every graph replay
-    if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
+    if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
     VolArgs vs = v;
     v.kchunk = s->kchunk;
     v.ctl_err = &s->ctl->err;
@@ -215,7 +224,7 @@ void enqueue_step(cgfd_solver *s, int it) {
         switch (kind) {
           case 0:
             launch_volume_interior(vk, idir, jdir, kdir, mode, s->stream);
-            if (s->timing) cudaEventRecordWithFlags(s->ev_int[ip][stage], s->stream, cudaEventRecordExternal);
+            if (tm) cudaEventRecordWithFlags(s->ev_int[ip][stage], s->stream, cudaEventRecordExternal);
             break;
           case 1: launch_volume_shell(vk, idir, jdir, kdir, mode, s->stream); break;
           case 2: launch_volume_face_x(vk, idir, jdir, kdir, mode, s->stream); break;
@@ -225,7 +234,7 @@ void enqueue_step(cgfd_solver *s, int it) {
         nl += vk.nbox > 0;
       }
     }
-    if (s->timing) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
+    if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
   }
   launch_advance(s->ctl, s->st.max_rec, s->stream);
   nl++;
@@ -255,7 +264,7 @@ void cgfd_config_default(cgfd_config *c) {
   }
 }
 
-const char *cgfd_last_error(void) { return g_err.c_str(); }
+const char *cgfd_last_error(void) { return g_err_is_fixed ? g_err_fixed : g_err.c_str(); }
 
 int cgfd_prepare(const cgfd_config *cfg, cgfd_setup **out) {
   if (!cfg || !out) return fail(CGFD_ERR_ARG, "null argument");
@@ -557,6 +566,71 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   if (c.it != s->it) return fail(CGFD_ERR_STATE, "device step counter out of step with the host");
   if (c.err & CTL_ERR_TMA) return fail(CGFD_ERR_CUDA, "volume kernel: a TMA row load did not complete in time");
   if (c.err & CTL_ERR_NONFINITE) return fail(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
+  return CGFD_OK;
+}
+
+// ---- cgfd_run_noalloc ------------------------------------------------------
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::atomic<float *> g_noalloc_ptr[kNoallocMaxDevices];
+
+int fail_fixed(int code, const char *m) {
+  size_t n = 0;
+  for (; m[n] && n + 1 < sizeof g_err_fixed; n++) g_err_fixed[n] = m[n];
+  g_err_fixed[n] = 0;
+  g_err_is_fixed = true;
+  return code;
+}
+
+int fail_fixed_cuda(cudaError_t e, const char *what) {
+  char b[sizeof g_err_fixed];
+  std::snprintf(b, sizeof b, "%s: %s", what, cudaGetErrorString(e));
+  return fail_fixed(e == cudaErrorMemoryAllocation ? CGFD_ERR_NOMEM : CGFD_ERR_CUDA, b);
+}
+}  // namespace
+
+int cgfd_run_noalloc(cgfd_solver *s, int nsteps) {
+  if (!s || nsteps < 0) return fail_fixed(CGFD_ERR_ARG, "bad argument");
+  // the largest fault's traction scratch must fit the static array
+  for (const FaultState &F : s->faults) {
+    if (F.nj <= 0 || F.nk <= 0) continue;
+    const unsigned long long need = 12ull * 9 * (F.nj + 6) * (F.nk + 6);
+    if (need > CGFD_NOALLOC_SCRATCH_FLOATS) {
+      char b[sizeof g_err_fixed];
+      std::snprintf(b, sizeof b,
+                    "cgfd_run_noalloc: the fault's split box needs %llu scratch floats, the static array holds %u",
+                    need, CGFD_NOALLOC_SCRATCH_FLOATS);
+      return fail_fixed(CGFD_ERR_ARG, b);
+    }
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: current device");
+  if (dev < 0 || dev >= kNoallocMaxDevices) return fail_fixed(CGFD_ERR_ARG, "cgfd_run_noalloc: device ordinal too large");
+  float *trac = g_noalloc_ptr[dev].load();
+  if (!trac) {
+    e = noalloc_scratch_address(&trac);
+    if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: scratch address");
+    g_noalloc_ptr[dev].store(trac);
+  }
+  long long nl = 0;
+  for (int q = 0; q < nsteps; q++) {
+    enqueue_step(s, s->it, trac, false);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: launch");
+    nl += s->launches_per_step;
+    s->it++;
+  }
+  s->last_launches = nl;
+  e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: run");
+  Ctl c;
+  e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: read control block");
+  if (c.it != s->it) return fail_fixed(CGFD_ERR_STATE, "device step counter out of step with the host");
+  if (c.err & CTL_ERR_TMA) return fail_fixed(CGFD_ERR_CUDA, "volume kernel: a TMA row load did not complete in time");
+  if (c.err & CTL_ERR_NONFINITE) return fail_fixed(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
   return CGFD_OK;
 }
 

@@ -226,6 +226,46 @@ int cgfd_last_timing(const cgfd_solver *s, double *run_ms, double *volume_ms,
 int cgfd_last_kernel_timing(const cgfd_solver *s, int which, double *ms,
                             long long *launches, long long *points);
 
+/* Advance nsteps time steps exactly like cgfd_run, allocating nothing
+ * (no counterpart in the reference).
+ *
+ * For callers that cannot allocate between steps.  Examples: a loop that
+ * shares the device with other work under a fixed memory budget, where
+ * every byte is already claimed.  Or a time-sliced loop that interleaves
+ * this solver with other GPU work and cannot afford the device-wide
+ * synchronisation that cudaMalloc / cudaFree may imply.  cgfd_run does
+ * allocate on first use: each of the 8 operator pairs is captured once as a
+ * CUDA graph, and instantiating a graph allocates host and device memory.
+ * This entry point instead launches the kernels of each step directly on
+ * the solver's stream.  It calls no allocating CUDA or library routine,
+ * and its error messages go to a fixed per-thread buffer.
+ *
+ * Scratch.  The fault kernels need one scratch buffer per RK stage (the
+ * tractions around the split nodes).  Here it is a fixed device array of
+ * CGFD_NOALLOC_SCRATCH_FLOATS floats (32 MiB), one per device, in the
+ * library's static device memory.  Each fault needs
+ * 108 * (nj_split + 6) * (nk_split + 6) floats, where nj_split x nk_split
+ * is the bounding box of its split nodes.  A solver whose fault needs more
+ * is rejected with CGFD_ERR_ARG before anything runs.  Faults are processed
+ * one after another, so the largest one sets the need.  Nothing in the
+ * array has to start at zero: every stage writes each element it reads.
+ *
+ * Set-up.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress).  That may also load the library's device code
+ * for that device.  Make this first call before any stream capture.  Call
+ * with the solver's device current, as for every entry point.
+ *
+ * Concurrency.  The array is shared by all solvers on a device.  Calls on
+ * the same device must not overlap: not from two threads, and not on two
+ * streams.  Overlapping calls race on the scratch and corrupt both results.
+ * Calls on different devices are independent.  Mixing cgfd_run and
+ * cgfd_run_noalloc on one solver is allowed; the state carries over.
+ *
+ * Returns like cgfd_run: CGFD_ERR_UNSTABLE on a non-finite slip rate or
+ * station value, CGFD_ERR_CUDA on a launch failure. */
+#define CGFD_NOALLOC_SCRATCH_FLOATS (8u * 1024u * 1024u)
+int cgfd_run_noalloc(cgfd_solver *s, int nsteps);
+
 /* Release device and host memory of the handle. */
 void cgfd_destroy(cgfd_solver *s);
 
