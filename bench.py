@@ -39,7 +39,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hills", choices=["hills", "hills_medium", "tpv"])
@@ -81,34 +81,58 @@ def allmax(ws, x):
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed
-    region."""
+    """nvidia-smi samples (every 200 ms) of SM clock, power and throttle
+    reasons; stop() keeps the samples taken inside the timed region."""
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.FIELDS}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 
-    def stop(self):
+    def wait_first_sample(self, timeout_s=10.0):
+        """Block until nvidia-smi has written a sample (it takes up to a
+        second to start), so that the timed region is covered."""
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < timeout_s:
+            if os.path.getsize(self.f.name) > 0:
+                return True
+            time.sleep(0.05)
+        return False
+
+    @staticmethod
+    def _stamp(t):
+        import datetime
+        try:
+            return datetime.datetime.strptime(t.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
+    def stop(self, t_start=None, t_end=None):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
         self.p.terminate()
         self.p.wait()
         self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 9]
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 10]
         os.unlink(self.f.name)
+        if t_start is not None:
+            inside = [r for r in rows if (self._stamp(r[0]) or 0) >= t_start - 0.2 and
+                      (self._stamp(r[0]) or 0) <= t_end + 0.2]
+            rows = inside or rows
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        load = [r for r in rows if r[4].strip().isdigit() and int(r[4]) >= 50] or rows
-        sm = [float(r[1]) for r in load if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        reasons = sorted({n for r in load for n, v in zip(names, r[6:10]) if v.strip() == "Active"})
+        load = [r for r in rows if r[5].strip().isdigit() and int(r[5]) >= 50] or rows
+        sm = [float(r[2]) for r in load if r[2].strip().replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit()]
+        reasons = sorted({n for r in load for n, v in zip(names, r[7:11]) if v.strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows), "samples_under_load": len(load)}
 
@@ -191,14 +215,17 @@ def main():
     torch.cuda.set_device(local)
     setup = cgfd.Setup(prob)
     s = cgfd.Solver(prob, setup=setup)
+    clk = ClockSampler(local)
     s.run(args.warmup)
     s.set_timing(True)
+    clk.wait_first_sample()
     barrier(ws)
     torch.cuda.synchronize()
-    clk = ClockSampler(local)
+    t_start = time.time()
     s.run(args.steps)
     torch.cuda.synchronize()
-    clocks = clk.stop()
+    t_end = time.time()
+    clocks = clk.stop(t_start, t_end)
     barrier(ws)
     run_ms, vol_ms, vol_n = s.last_timing()
     int_ms, int_n, int_pts = s.kernel_timing(1)

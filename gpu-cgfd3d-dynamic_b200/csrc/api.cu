@@ -507,10 +507,34 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   double vol_ms = 0, int_ms = 0;
   long long vol_n = 0, int_n = 0;
   const bool int_timed = s->tiled == 0 && s->nkbox[0] > 0;
+  // with timing on, the events of step it (recorded by the graph of it % 8)
+  // are read just before that graph is launched again 8 steps later, and
+  // the last 8 after the loop: the host never waits on the step in flight
+  auto read_events = [&](int it) -> cudaError_t {
+    cudaError_t er = cudaEventSynchronize(s->ev_vol[it % 8][3][1]);
+    if (er != cudaSuccess) return er;
+    for (int st = 0; st < 4; st++) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, s->ev_vol[it % 8][st][0], s->ev_vol[it % 8][st][1]);
+      vol_ms += ms;
+      vol_n++;
+      if (int_timed) {
+        cudaEventElapsedTime(&ms, s->ev_vol[it % 8][st][0], s->ev_int[it % 8][st]);
+        int_ms += ms;
+        int_n++;
+      }
+    }
+    return cudaSuccess;
+  };
+  const int it0 = s->it;
   cudaError_t e = cudaEventRecord(s->ev_run[0], s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "event");
   for (int q = 0; q < nsteps; q++) {
     const int it = s->it;
+    if (s->timing && it - 8 >= it0) {
+      e = read_events(it - 8);
+      if (e != cudaSuccess) return cuda_fail(e, "timing");
+    }
     if (s->use_graph) {
       cudaGraphExec_t &G = s->graph[s->timing][it % 8];
       if (!G) {
@@ -531,28 +555,17 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "launch");
     }
-    if (s->timing) {
-      // the events of this step are reused by the next step of the same
-      // operator pair, so read them now
-      e = cudaEventSynchronize(s->ev_vol[it % 8][3][1]);
-      if (e != cudaSuccess) return cuda_fail(e, "timing");
-      for (int st = 0; st < 4; st++) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, s->ev_vol[it % 8][st][0], s->ev_vol[it % 8][st][1]);
-        vol_ms += ms;
-        vol_n++;
-        if (int_timed) {
-          cudaEventElapsedTime(&ms, s->ev_vol[it % 8][st][0], s->ev_int[it % 8][st]);
-          int_ms += ms;
-          int_n++;
-        }
-      }
-    }
     nl += s->launches_per_step;
     s->it++;
   }
   e = cudaEventRecord(s->ev_run[1], s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "event");
+  if (s->timing) {
+    for (int it = std::max(it0, s->it - 8); it < s->it; it++) {
+      e = read_events(it);
+      if (e != cudaSuccess) return cuda_fail(e, "timing");
+    }
+  }
   s->last_launches = nl;
   e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "run");

@@ -243,8 +243,22 @@ __device__ __forceinline__ bool locate(const VolArgs &a, int &i, int &j, int &k)
   return i <= B.i1 && j <= B.j1 && k <= B.k1;
 }
 
+// resident blocks per SM asked of the compiler, per kernel kind (register
+// budget 65536 / (256 x blocks))
+#ifndef CGFD_LB_INTERIOR
+#define CGFD_LB_INTERIOR 4
+#endif
+#ifndef CGFD_LB_SHELL
+#define CGFD_LB_SHELL 3
+#endif
+#ifndef CGFD_LB_FACE
+#define CGFD_LB_FACE 3
+#endif
+
 template <int ID, int JD, int KD, int MODE, int KIND>
-__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? 4 : 3) k_volume(const __grid_constant__ VolArgs a) {
+__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
+                                         : (KIND == SHELL ? CGFD_LB_SHELL : CGFD_LB_FACE))
+    k_volume(const __grid_constant__ VolArgs a) {
   static_assert(KIND >= INTERIOR && KIND <= FACE_Z, "kernel kind");
   const Grid &g = a.g;
   int i, j, k;

@@ -211,7 +211,8 @@ int cgfd_restore(cgfd_solver *s, const void *buf, unsigned long long bytes);
 int cgfd_last_launches(const cgfd_solver *s, long long *launches);
 
 /* 1: time every volume-stage launch with CUDA events on the solver's
- * stream (cgfd_run then waits for each step); 0: off (default). */
+ * stream (cgfd_run reads each step's events 8 steps later, so the host
+ * never waits on the step in flight); 0: off (default). */
 int cgfd_set_timing(cgfd_solver *s, int on);
 /* Device time of the last cgfd_run (events on the solver's stream at its
  * start and end) and, with timing on, the summed duration and count of its
