@@ -23,14 +23,16 @@
 #include "setup.h"
 
 namespace cgfd {
-void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, int bz);
-int volume_interior_bz();
+void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, bool pack);
 void launch_volume_interior(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_shell(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_x(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void volume_zq_layout(VolArgs &a, const int box[6], int kchunk);
+cudaError_t volume_sm_prepare();
+void volume_sm_layout(VolArgs &a, const int box[6], int kchunk);
+void launch_volume_sm(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_zq(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void volume_tma_prepare();
 int volume_tma_encode(CUtensorMap *tm, const float *level, const Grid &g);
@@ -102,6 +104,8 @@ struct cgfd_solver {
   long long launches_per_step = 0, last_launches = 0;
   int tiled = 0, kchunk = 32;           // volume kernels: 0 boxes, 2 TMA-fed, 3 z-marching interior + boxes
   int kchunk_zq = 32;
+  int ychunk = 16;                      // interior kernel: y tiles per z-marching chunk
+  bool pack = true;                     // pack boxes at most 24 points wide (x PML slabs)
   int kchunk_tma = 32;
   int box_top[1][6];                    // rows under the free surface
   CUtensorMap tmap[4];                  // TMA maps of the 4 level slots
@@ -203,7 +207,7 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       v.kend = s->isfree ? s->g.nk - 4 : s->g.nk;
       v.kchunk = s->kchunk_tma;
       launch_volume_tma(s->tmap[scur], v, idir, jdir, kdir, mode, s->stream);
-      volume_boxes(vs, s->box_top, 1, 1);
+      volume_boxes(vs, s->box_top, 1, true);
       launch_volume_shell(vs, idir, jdir, kdir, mode, s->stream);
       nl += 1 + (vs.nbox > 0);
     } else {
@@ -216,10 +220,18 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
         launch_volume_zq(vz, idir, jdir, kdir, mode, s->stream);
         nl += vz.nbox > 0;
         kind0 = 1;
+      } else if (s->tiled == 4) {
+        VolArgs vz = v;
+        volume_sm_layout(vz, s->box_in[0], s->kchunk_zq);
+        launch_volume_sm(vz, idir, jdir, kdir, mode, s->stream);
+        if (tm) cudaEventRecordWithFlags(s->ev_int[ip][stage], s->stream, cudaEventRecordExternal);
+        nl += vz.nbox > 0;
+        kind0 = 1;
       }
       for (int kind = kind0; kind < 5; kind++) {
         VolArgs vk = vs;
-        volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind == 0 ? volume_interior_bz() : 1);
+        volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind != 0 && s->pack);
+        vk.ychunk = s->ychunk;
         if (vk.nbox == 0) continue;
         switch (kind) {
           case 0:
@@ -331,6 +343,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   s->tiled = 0;
   if (vk && std::strcmp(vk, "tma") == 0) s->tiled = 2;
   if (vk && std::strcmp(vk, "zq") == 0) s->tiled = 3;
+  if (vk && std::strcmp(vk, "sm") == 0) s->tiled = 4;
   {
     // z chunk per block: enough blocks for several waves, rows >= 8
     const long bxy = (long)((H.g.ni + 31) / 32) * ((H.g.nj + 7) / 8);
@@ -343,6 +356,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   const size_t lev = (size_t)NCMP * g.scmp, ns = (size_t)g.ny * g.nz;
 #define CK(x, what) do { cudaError_t _e = (x); if (_e != cudaSuccess) { destroy(s); return cuda_fail(_e, what); } } while (0)
   for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
+  if (s->tiled == 4) CK(volume_sm_prepare(), "shared-memory attribute");
   if (s->tiled == 2) {
     volume_tma_prepare();
     for (int L = 0; L < 4; L++)
@@ -469,6 +483,11 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     const long nz = std::max(1, khi - klo + 1);
     const long nch = std::max<long>(1, (8L * 2 * nsm + tiles - 1) / std::max<long>(1, tiles));
     s->kchunk_zq = (int)std::max<long>(16, (nz + nch - 1) / nch);
+    const char *pk = std::getenv("CGFD_PACK");
+    if (pk && pk[0] == '0') s->pack = false;
+    const char *yc = std::getenv("CGFD_INTERIOR_YCHUNK");
+    if (yc && std::atoi(yc) > 0) s->ychunk = std::atoi(yc);
+    s->ychunk = std::min(s->ychunk, std::max(1, (jhi - jlo + 8) / 8));
     const char *kc = std::getenv("CGFD_ZQ_KCHUNK");
     if (kc && std::atoi(kc) > 0) s->kchunk_zq = std::atoi(kc);
     // points one interior launch / one volume stage updates: the split-node
@@ -506,7 +525,7 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   long long nl = 0;
   double vol_ms = 0, int_ms = 0;
   long long vol_n = 0, int_n = 0;
-  const bool int_timed = s->tiled == 0 && s->nkbox[0] > 0;
+  const bool int_timed = (s->tiled == 0 || s->tiled == 4) && s->nkbox[0] > 0;
   // with timing on, the events of step it (recorded by the graph of it % 8)
   // are read just before that graph is launched again 8 steps later, and
   // the last 8 after the loop: the host never waits on the step in flight
@@ -542,7 +561,14 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
         e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_fail(e, "begin capture");
         enqueue_step(s, it);
+        // a launch refused during capture (bad configuration) is not part
+        // of the graph and would otherwise go unnoticed
+        const cudaError_t le = cudaGetLastError();
         e = cudaStreamEndCapture(s->stream, &gr);
+        if (le != cudaSuccess) {
+          if (e == cudaSuccess) cudaGraphDestroy(gr);
+          return cuda_fail(le, "launch");
+        }
         if (e != cudaSuccess) return cuda_fail(e, "end capture");
         e = cudaGraphInstantiate(&G, gr, 0);
         cudaGraphDestroy(gr);

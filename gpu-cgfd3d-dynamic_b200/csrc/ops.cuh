@@ -73,6 +73,7 @@ struct VolArgs {
   int kend;                    // rows [0, kend) handled by the TMA kernel
   int *ctl_err;                // Ctl::err of the solver
   int nbox, nblocks;
+  int ychunk;                  // interior kernel: y tiles per chunk (z marches within a chunk)
   VolBox box[12];
   const float *cur, *pre;
   float *out, *end;            // next-stage level (null at the last stage), E

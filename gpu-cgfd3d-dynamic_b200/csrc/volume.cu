@@ -37,12 +37,7 @@ namespace cgfd {
 namespace {
 
 constexpr int BX = 32, BY = 8;
-// z rows per block of the interior kernel (blocks of 32 x 8/IBZ x IBZ):
-// taps along z of neighbouring rows then meet in L1
-#ifndef CGFD_INTERIOR_BZ
-#define CGFD_INTERIOR_BZ 1
-#endif
-constexpr int IBZ = CGFD_INTERIOR_BZ;
+
 
 // conservative traction J * (e . sigma_row) at point q for metric row `ax`
 // (MXIX, METX or MZTX) and stress row r (0: xx,xy,xz; 1: xy,yy,yz;
@@ -217,9 +212,7 @@ __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float 
 enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4 };
 
 // block -> point; boxes with a narrow x extent (PML x slabs) pack their
-// points densely instead of leaving most of a 32-wide row idle; blocks of
-// the interior kernel cover BZ z rows (threadIdx.z)
-template <int BZ>
+// points densely instead of leaving most of a 32-wide row idle
 __device__ __forceinline__ bool locate(const VolArgs &a, int &i, int &j, int &k) {
   int b = 0;
 #pragma unroll 1
@@ -238,9 +231,24 @@ __device__ __forceinline__ bool locate(const VolArgs &a, int &i, int &j, int &k)
   }
   const int bx = bid % B.nbx, rem = bid / B.nbx, by = rem % B.nby, bz = rem / B.nby;
   i = B.i0 + bx * BX + threadIdx.x;
-  j = B.j0 + by * (BY / BZ) + threadIdx.y;
-  k = B.k0 + bz * BZ + threadIdx.z;
-  return i <= B.i1 && j <= B.j1 && k <= B.k1;
+  j = B.j0 + by * BY + threadIdx.y;
+  k = B.k0 + bz;
+  return i <= B.i1 && j <= B.j1;
+}
+
+// interior box (one box): 3-D grid (x tiles, y tiles of one chunk, z rows x
+// chunks).  The blocks of one y chunk of a.ychunk tiles march up z before
+// the next chunk starts, so the planes a z window touches stay in L2 (a
+// whole xy plane per z row would need more than the 126 MB L2 holds).
+__device__ __forceinline__ bool locate_interior(const VolArgs &a, int &i, int &j, int &k) {
+  const VolBox &B = a.box[0];
+  const int nkb = B.k1 - B.k0 + 1;
+  const int chunk = blockIdx.z / nkb, bz = blockIdx.z - chunk * nkb;
+  const int by = chunk * a.ychunk + blockIdx.y;
+  i = B.i0 + blockIdx.x * BX + threadIdx.x;
+  j = B.j0 + by * BY + threadIdx.y;
+  k = B.k0 + bz;
+  return i <= B.i1 && j <= B.j1;
 }
 
 // resident blocks per SM asked of the compiler, per kernel kind (register
@@ -262,7 +270,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   static_assert(KIND >= INTERIOR && KIND <= FACE_Z, "kernel kind");
   const Grid &g = a.g;
   int i, j, k;
-  if (!locate<KIND == INTERIOR ? IBZ : 1>(a, i, j, k)) return;
+  if (KIND == INTERIOR ? !locate_interior(a, i, j, k) : !locate(a, i, j, k)) return;
   const int I = i + NG, J = j + NG, K = k + NG;
   // split-node slabs (i0-3..i0+3 of unwelded nodes) belong to the fault kernels
   for (int f = 0; f < a.nfault; f++) {
@@ -424,9 +432,13 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
 template <int ID, int JD, int KD, int KIND>
 void launch4(const VolArgs &a, int mode, cudaStream_t st) {
   if (a.nbox == 0) return;
-  constexpr int BZ = KIND == INTERIOR ? IBZ : 1;
-  const dim3 blk(BX, BY / BZ, BZ);
-  const dim3 grd(a.nblocks);
+  const dim3 blk(BX, BY, 1);
+  dim3 grd(a.nblocks);
+  if (KIND == INTERIOR) {
+    const VolBox &B = a.box[0];
+    const int nchunks = (B.nby + a.ychunk - 1) / a.ychunk;
+    grd = dim3(B.nbx, a.ychunk, (B.k1 - B.k0 + 1) * nchunks);
+  }
   if (mode == RK_FIRST) k_volume<ID, JD, KD, RK_FIRST, KIND><<<grd, blk, 0, st>>>(a);
   else if (mode == RK_MID) k_volume<ID, JD, KD, RK_MID, KIND><<<grd, blk, 0, st>>>(a);
   else k_volume<ID, JD, KD, RK_LAST, KIND><<<grd, blk, 0, st>>>(a);
@@ -456,9 +468,10 @@ void launch_kind(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaS
 #endif
 
 #if CGFD_VOLUME_KIND == 0
-// boxes (interior indices, inclusive) -> block layout of one launch; boxes
-// at most 24 points wide in x are packed (nbx = 0)
-void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, int bz) {
+// boxes (interior indices, inclusive) -> block layout of one launch; with
+// pack, boxes at most 24 points wide in x are packed (nbx = 0); the
+// interior kernel's 3-D grid needs the tiled layout (pack = false)
+void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, bool pack) {
   a.nbox = 0;
   int first = 0;
   for (int q = 0; q < n; q++) {
@@ -467,12 +480,7 @@ void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, int bz) {
     VolBox &B = a.box[a.nbox++];
     B.i0 = b[0]; B.i1 = b[1]; B.j0 = b[2]; B.j1 = b[3]; B.k0 = b[4]; B.k1 = b[5];
     const int ni = b[1] - b[0] + 1, nj = b[3] - b[2] + 1, nk = b[5] - b[4] + 1;
-    if (bz > 1) {
-      B.nbx = (ni + BX - 1) / BX;
-      B.nby = (nj + BY / bz - 1) / (BY / bz);
-      B.first = first;
-      first += B.nbx * B.nby * ((nk + bz - 1) / bz);
-    } else if (ni <= 24) {
+    if (pack && ni <= 24) {
       B.nbx = 0;
       B.nby = (ni * nj + BX * BY - 1) / (BX * BY);
       B.first = first;
@@ -486,8 +494,6 @@ void volume_boxes(VolArgs &a, const int (*boxes)[6], int n, int bz) {
   }
   a.nblocks = first;
 }
-
-int volume_interior_bz() { return IBZ; }
 
 void launch_volume_interior(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
   launch_kind<INTERIOR>(a, idir, jdir, kdir, mode, st);
