@@ -244,7 +244,11 @@ int cgfd_last_kernel_timing(const cgfd_solver *s, int which, double *ms,
  * Scratch.  The fault kernels need one scratch buffer per RK stage (the
  * tractions around the split nodes).  Here it is a fixed device array of
  * CGFD_NOALLOC_SCRATCH_FLOATS floats (32 MiB), one per device, in the
- * library's static device memory.  Each fault needs
+ * library's static device memory: a GPU holds those 32 MiB from the time
+ * the CUDA runtime loads this part of the library's device code on it (at
+ * the latest, the first call of this entry point on that GPU; with eager
+ * module loading, when the library's context starts) until the process
+ * exits.  Each fault needs
  * 108 * (nj_split + 6) * (nk_split + 6) floats, where nj_split x nk_split
  * is the bounding box of its split nodes.  A solver whose fault needs more
  * is rejected with CGFD_ERR_ARG before anything runs.  Faults are processed
