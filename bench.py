@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hills", choices=["hills", "hills_medium", "tpv"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble", type=int, default=0, metavar="N",
+                    help="batched form: N seeded scenarios of uneven size advanced as one ensemble, against a "
+                         "loop of the plain solver over the same scenarios; prints scenarios/hour")
     ap.add_argument("--e2e-steps", type=int, default=0,
                     help="steps of the end-to-end run (default: max(--steps, 100), so that the one-time upload "
                          "is amortised over a run of realistic length)")
@@ -186,8 +189,58 @@ def oracle_rate(prob, steps, warmup, budget_s=150.0):
     return prob.points / one / 1e9, th, f"{n} full time step(s) of the same problem after set-up, {th} OpenMP threads"
 
 
+def ensemble_main(args):
+    """Scenarios per hour of 1500-step runs, from --steps timed steps of
+    every scenario: the ensemble (one graph launch per step, a branch per
+    scenario) against looping cgfd_run over the same solvers."""
+    import torch
+    import cgfd
+    import inputs
+    torch.cuda.set_device(0)
+    probs = inputs.ensemble_scenarios(args.ensemble, nt=args.warmup + 2 * args.steps + 16)
+    solvers = [cgfd.Solver(p) for p in probs]
+    pts = sum(p.points for p in probs)
+    for s in solvers:                              # warm-up: graphs of every operator pair
+        s.run(max(args.warmup, 8))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in solvers:
+        s.run(args.steps)
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter() - t0
+    ens = cgfd.Ensemble(solvers)
+    ens.run(8)
+    torch.cuda.synchronize()
+    clk = ClockSampler(0)
+    clk.wait_first_sample()
+    t_start = time.time()
+    t0 = time.perf_counter()
+    ens.run(args.steps)
+    torch.cuda.synchronize()
+    t_ens = time.perf_counter() - t0
+    clocks = clk.stop(t_start, time.time())
+    full = 1500
+    rate = lambda t: len(probs) * 3600.0 / (t * full / args.steps)
+    line = {"metric": "ensemble scenarios/hour", "value": rate(t_ens), "unit": "scenarios/h",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(probs)} seeded scenarios (inputs.ensemble_scenarios): grids "
+                                   "64-160 x 96-256 x 64-128, h 100-200 m, von Karman shear stress, random "
+                                   "nucleation, mu_s 0.6-0.7, Dc 0.2-0.5 m, half with hill topography; "
+                                   f"{full}-step runs, rate from {args.steps} timed steps of every scenario",
+                       "points": pts},
+            "loop": {"value": rate(t_loop), "unit": "scenarios/h",
+                     "note": "cgfd_run over the same solvers one after another"},
+            "speedup_vs_loop": t_loop / t_ens,
+            "gpt_per_s": pts * args.steps / t_ens / 1e9, "clocks": clocks}
+    ens.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.ensemble:
+        return ensemble_main(args)
     ws, rank, local = dist_init()
     prob, desc = make_problem(args.workload)
     metric, unit = "Gpt-updates/s", "Gpt/s"

@@ -222,6 +222,10 @@ def load_library(path: str = LIB_PATH):
     lib.cgfd_set_timing.argtypes = [vp, C.c_int]
     lib.cgfd_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     lib.cgfd_run_noalloc.argtypes = [vp, C.c_int]
+    lib.cgfd_ensemble_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
+    lib.cgfd_ensemble_run.argtypes = [vp, C.c_int]
+    lib.cgfd_ensemble_destroy.argtypes = [vp]
+    lib.cgfd_ensemble_destroy.restype = None
     lib.cgfd_last_kernel_timing.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                             C.POINTER(C.c_longlong)]
     _lib = lib
@@ -391,6 +395,38 @@ class Solver:
     def close(self):
         if getattr(self, "h", None):
             self.lib.cgfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Ensemble:
+    """Independent solvers advanced together, one CUDA graph per step with a
+    branch per member (cgfd_ensemble_*).  The members stay usable through
+    their own getters; keep them alive while the ensemble exists."""
+
+    def __init__(self, solvers):
+        self.lib = load_library()
+        self.members = list(solvers)
+        arr = (C.c_void_p * len(self.members))(*[m.h for m in self.members])
+        h = C.c_void_p()
+        rc = self.lib.cgfd_ensemble_create(arr, len(self.members), C.byref(h))
+        if rc != 0:
+            raise CgfdError(f"{ERRORS.get(rc, rc)}: {self.lib.cgfd_last_error().decode()}")
+        self.h = h
+
+    def run(self, nsteps: int):
+        rc = self.lib.cgfd_ensemble_run(self.h, int(nsteps))
+        if rc != 0:
+            raise CgfdError(f"{ERRORS.get(rc, rc)}: {self.lib.cgfd_last_error().decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cgfd_ensemble_destroy(self.h)
             self.h = None
 
     def __del__(self):

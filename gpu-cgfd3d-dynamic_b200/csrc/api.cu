@@ -673,6 +673,100 @@ int cgfd_run_noalloc(cgfd_solver *s, int nsteps) {
   return CGFD_OK;
 }
 
+// ---- ensembles ---------------------------------------------------------------
+struct cgfd_ensemble {
+  std::vector<cgfd_solver *> m;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t graph[8] = {};
+};
+
+static void ensemble_free(cgfd_ensemble *e) {
+  if (!e) return;
+  for (int q = 0; q < 8; q++) if (e->graph[q]) cudaGraphExecDestroy(e->graph[q]);
+  for (cudaEvent_t ev : e->join) if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->origin) cudaStreamDestroy(e->origin);
+  delete e;
+}
+
+int cgfd_ensemble_create(cgfd_solver *const *members, int n, cgfd_ensemble **out) {
+  if (!members || n <= 0 || !out) return fail(CGFD_ERR_ARG, "bad argument");
+  *out = nullptr;
+  for (int q = 0; q < n; q++) {
+    if (!members[q]) return fail(CGFD_ERR_ARG, "null ensemble member");
+    if (members[q]->it != members[0]->it) return fail(CGFD_ERR_STATE, "ensemble members at different steps");
+    for (int r = 0; r < q; r++)
+      if (members[r] == members[q]) return fail(CGFD_ERR_ARG, "solver given twice to an ensemble");
+  }
+  cgfd_ensemble *e = new cgfd_ensemble();
+  e->m.assign(members, members + n);
+  cudaError_t er = cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking);
+  if (er == cudaSuccess) er = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+  e->join.assign(n, nullptr);
+  for (int q = 0; q < n && er == cudaSuccess; q++) er = cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming);
+  if (er != cudaSuccess) { ensemble_free(e); return cuda_fail(er, "ensemble set-up"); }
+  *out = e;
+  return CGFD_OK;
+}
+
+int cgfd_ensemble_run(cgfd_ensemble *e, int nsteps) {
+  if (!e || nsteps < 0) return fail(CGFD_ERR_ARG, "bad argument");
+  const int n = (int)e->m.size();
+  for (int q = 1; q < n; q++)
+    if (e->m[q]->it != e->m[0]->it) return fail(CGFD_ERR_STATE, "ensemble members out of step (cgfd_run on a member?)");
+  cudaError_t er;
+  for (int step = 0; step < nsteps; step++) {
+    const int it = e->m[0]->it;
+    cudaGraphExec_t &G = e->graph[it % 8];
+    if (!G) {
+      // fork from the origin stream to every member's stream, one step of
+      // each member, join back: a graph with one branch per member
+      cudaGraph_t gr;
+      er = cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal);
+      if (er != cudaSuccess) return cuda_fail(er, "begin ensemble capture");
+      cudaEventRecord(e->fork, e->origin);
+      for (int q = 0; q < n; q++) {
+        cgfd_solver *s = e->m[q];
+        cudaStreamWaitEvent(s->stream, e->fork, 0);
+        enqueue_step(s, it, nullptr, false);
+        cudaEventRecord(e->join[q], s->stream);
+        cudaStreamWaitEvent(e->origin, e->join[q], 0);
+      }
+      const cudaError_t le = cudaGetLastError();
+      er = cudaStreamEndCapture(e->origin, &gr);
+      if (le != cudaSuccess) {
+        if (er == cudaSuccess) cudaGraphDestroy(gr);
+        return cuda_fail(le, "ensemble launch");
+      }
+      if (er != cudaSuccess) return cuda_fail(er, "end ensemble capture");
+      er = cudaGraphInstantiate(&G, gr, 0);
+      cudaGraphDestroy(gr);
+      if (er != cudaSuccess) { G = nullptr; return cuda_fail(er, "instantiate ensemble graph"); }
+    }
+    er = cudaGraphLaunch(G, e->origin);
+    if (er != cudaSuccess) return cuda_fail(er, "ensemble graph launch");
+    for (cgfd_solver *s : e->m) { s->it++; s->last_launches = 0; }
+  }
+  er = cudaStreamSynchronize(e->origin);
+  if (er != cudaSuccess) return cuda_fail(er, "ensemble run");
+  for (int q = 0; q < n; q++) {
+    cgfd_solver *s = e->m[q];
+    s->last_launches = (long long)nsteps * s->launches_per_step;
+    Ctl c;
+    er = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
+    if (er != cudaSuccess) return cuda_fail(er, "read control block");
+    const std::string who = "ensemble member " + std::to_string(q) + ": ";
+    if (c.it != s->it) return fail(CGFD_ERR_STATE, who + "device step counter out of step with the host");
+    if (c.err & CTL_ERR_TMA) return fail(CGFD_ERR_CUDA, who + "volume kernel: a TMA row load did not complete in time");
+    if (c.err & CTL_ERR_NONFINITE) return fail(CGFD_ERR_UNSTABLE, who + "non-finite slip rate or station value");
+  }
+  return CGFD_OK;
+}
+
+void cgfd_ensemble_destroy(cgfd_ensemble *e) { ensemble_free(e); }
+
 int cgfd_set_timing(cgfd_solver *s, int on) {
   if (!s) return fail(CGFD_ERR_ARG, "bad argument");
   s->timing = on ? 1 : 0;

@@ -185,3 +185,100 @@ def small_planar(seed=7, dynamic_method=2, free_surface=1, pml=5, nt=60, **kw):
                 margin=10, dynamic_method=dynamic_method, free_surface=free_surface)
     args.update(kw)
     return tpv_planar(**args)
+
+
+def von_karman(nj, nk, h, corr=2000.0, hurst=0.8, rng=None):
+    """Zero-mean, unit-variance 2-D random field [nk, nj] with a von Karman
+    spectrum P(k) ~ (1 + k^2 a^2)^-(H + 1) (correlation length a, Hurst
+    exponent H), made by filtering white noise in the Fourier domain."""
+    rng = np.random.default_rng() if rng is None else rng
+    ky = 2.0 * np.pi * np.fft.fftfreq(nj, d=h)
+    kz = 2.0 * np.pi * np.fft.fftfreq(nk, d=h)
+    k2 = kz[:, None] ** 2 + ky[None, :] ** 2
+    amp = (1.0 + k2 * corr * corr) ** (-(hurst + 1.0) / 2.0)
+    f = np.real(np.fft.ifft2(np.fft.fft2(rng.standard_normal((nk, nj))) * amp))
+    f -= f.mean()
+    return f / max(f.std(), 1e-30)
+
+
+def _hill_coords(ni, nj, nk, h, nhills, rng):
+    """Curvilinear coordinates [nk, nj, ni] under a sum of Gaussian hills,
+    stretched linearly from a flat bottom; the fault plane is x = 0 at
+    i = ni // 2."""
+    xs = (np.arange(ni) - ni // 2) * h
+    ys = (np.arange(nj) - nj / 2.0) * h
+    X2, Y2 = np.meshgrid(xs, ys)
+    topo = np.zeros_like(X2)
+    for _ in range(nhills):
+        amp = rng.uniform(100.0, 800.0) * h / 100.0
+        sig = rng.uniform(2000.0, 6000.0) * h / 100.0
+        cx = rng.uniform(xs[0], xs[-1])
+        cy = rng.uniform(ys[0], ys[-1])
+        topo += amp * np.exp(-((X2 - cx) ** 2 + (Y2 - cy) ** 2) / (2 * sig * sig))
+    zb = -(nk - 1) * h
+    t = np.arange(nk) / (nk - 1.0)
+    z3 = zb + (topo[None] - zb) * t[:, None, None]
+    x3 = np.broadcast_to(X2[None], (nk, nj, ni))
+    y3 = np.broadcast_to(Y2[None], (nk, nj, ni))
+    return (np.ascontiguousarray(x3, np.float32), np.ascontiguousarray(y3, np.float32),
+            np.ascontiguousarray(z3, np.float32))
+
+
+def ensemble_scenarios(n=64, seed=1003, nt=1500, size_lo=(64, 96, 64), size_hi=(160, 256, 128),
+                       pml=10, margin=10, cfl=0.5):
+    """A seeded ensemble of rupture scenarios of uneven size (the batched
+    workload): per scenario the grid (fault-normal ni in [64, 160], strike
+    nj in [96, 256], depth nk in [64, 128]) and spacing h in [100, 200] m
+    are drawn uniformly; the medium is homogeneous (6000 / 3464 m/s,
+    2670 kg/m^3); the vertical fault at ni // 2 spans 75% of the strike and
+    the top 75% of the depth; the shear traction is a von Karman field
+    (correlation 2 km, Hurst 0.8, std 8 MPa, mean 60 MPa) kept below 95% of
+    the static strength, with a 7 x 7-node nucleation patch at a random
+    place raised 2 MPa above it; mu_s in [0.6, 0.7], mu_d 0.5, Dc in
+    [0.2, 0.5] m; half of the scenarios have Gaussian-hill topography, the
+    others a flat surface; 10-layer CFS-PML, free surface, dt at CFL 0.5."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        ni = int(rng.integers(size_lo[0], size_hi[0] + 1))
+        nj = int(rng.integers(size_lo[1], size_hi[1] + 1))
+        nk = int(rng.integers(size_lo[2], size_hi[2] + 1))
+        h = float(rng.uniform(100.0, 200.0))
+        mu_s = float(rng.uniform(0.6, 0.7))
+        dc = float(rng.uniform(0.2, 0.5))
+        hills = bool(rng.integers(0, 2))
+        lam, mu, rho = _homog(ni, nj, nk)
+        fg = [int(round(nj * 0.125)) + 1, int(round(nj * 0.875)) + 1, int(round(nk * 0.25)) + 1, nk]
+        j1, j2, k1, k2 = [v - 1 for v in fg]
+        strength = mu_s * 100.0
+        ts = 60.0 + 8.0 * von_karman(nj, nk, h, rng=rng)
+        ts = np.minimum(ts, 0.95 * strength)
+        jc = int(rng.integers(max(j1 + margin + 4, 3), max(j2 - margin - 3, j1 + margin + 5)))
+        kc = int(rng.integers(max(k1 + margin + 4, 3), max(nk - 5, k1 + margin + 5)))
+        ts[kc - 3:kc + 4, jc - 3:jc + 4] = strength + 2.0
+        st = _stress(nj, nk, fg, (jc, kc), 3, t_nuc=strength + 2.0, mu_s=mu_s, dc=dc,
+                     ts_field=ts * MPA)
+        P = ((pml, pml), (pml, pml), (pml, 0))
+        vp = float(np.sqrt((lam[0, 0, 0] + 2 * mu[0, 0, 0]) / rho[0, 0, 0]))
+        dt = float(f"{cfl * h / (math.sqrt(3.0) * vp):.3g}")
+        sta = np.stack([rng.integers(pml + 2, ni - pml - 2, 4), rng.integers(pml + 2, nj - pml - 2, 4),
+                        np.full(4, nk - 1)], 1).astype(np.float32)
+        geo = {}
+        if hills:
+            x3, y3, z3 = _hill_coords(ni, nj, nk, h, int(rng.integers(1, 4)), rng)
+            geo = dict(grid_mode=GRID_IMPORT, x3d=x3, y3d=y3, z3d=z3)
+        else:
+            jj, kk = np.meshgrid(np.arange(1, nj + 1), np.arange(1, nk + 1))
+            geo = dict(grid_mode=GRID_FAULT_PLANE, fault_interval=h,
+                       fault_x=np.zeros((1, nk, nj), np.float32),
+                       fault_y=((jj - nj / 2.0) * h).astype(np.float32)[None],
+                       fault_z=((kk - nk) * h).astype(np.float32)[None])
+        out.append(Problem(ni=ni, nj=nj, nk=nk, dt=dt, lam=lam, mu=mu, rho=rho,
+                           fault_x_index=[ni // 2 + 1], fault_grid=[fg],
+                           T0x=st[0][None], T0y=st[1][None], T0z=st[2][None], mu_s=st[3][None],
+                           mu_d=st[4][None], Dc=st[5][None], C0=st[6][None],
+                           dynamic_method=2, welded_margin=margin, free_surface=1,
+                           pml_layers=P, pml_ref_vel=((vp, vp),) * 3, stations=sta,
+                           fault_stations=np.array([[jc, kc]], np.float32), max_records=nt + 1,
+                           name=f"scenario_{q}_{nj}x{ni}x{nk}_{'hills' if hills else 'flat'}", **geo))
+    return out

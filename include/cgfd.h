@@ -271,6 +271,23 @@ int cgfd_last_kernel_timing(const cgfd_solver *s, int which, double *ms,
 #define CGFD_NOALLOC_SCRATCH_FLOATS (8u * 1024u * 1024u)
 int cgfd_run_noalloc(cgfd_solver *s, int nsteps);
 
+/* Ensembles (no counterpart in the reference: the batched-scenario form of
+ * the forward run).  A set of independent solvers, typically scenarios of
+ * different sizes, stress fields and nucleation points, advanced together:
+ * each time step of all members is one CUDA graph launch whose branches are
+ * the members' steps, each on its member's own stream, so that scenarios too
+ * small to fill the GPU alone run side by side.  Members stay owned by the
+ * caller, must live on the current device, must have taken the same number
+ * of steps, and must outlive the ensemble; read their results with the
+ * usual getters.  Calling cgfd_run on a member between ensemble runs puts
+ * it out of step: cgfd_ensemble_run then returns CGFD_ERR_STATE. */
+typedef struct cgfd_ensemble cgfd_ensemble;
+int cgfd_ensemble_create(cgfd_solver *const *members, int n, cgfd_ensemble **out);
+/* Advance every member by nsteps time steps.  Returns the first member
+ * error (CGFD_ERR_UNSTABLE, ...) with the member's index in the message. */
+int cgfd_ensemble_run(cgfd_ensemble *e, int nsteps);
+void cgfd_ensemble_destroy(cgfd_ensemble *e);
+
 /* Release device and host memory of the handle. */
 void cgfd_destroy(cgfd_solver *s);
 
