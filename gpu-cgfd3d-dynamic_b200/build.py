@@ -21,6 +21,9 @@ NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CU = [("volume.cu", f"volume_k{k}.cu.o", [f"-DCGFD_VOLUME_KIND={k}"]) for k in range(5)] + [
     (f, f + ".o", []) for f in ("volume_zq.cu", "volume_sm.cu", "volume_tma.cu", "fault.cu", "noalloc.cu", "api.cu")]
 CPP = ["setup.cpp"]
+DRIVER = os.path.join(HERE, "driver")
+DRIVER_SRC = ["cgfd_run.cpp", "ncclassic.cpp", "sac.cpp"]
+DRIVER_BIN = os.path.join(HERE, "lib", "cgfd_run")
 HEADERS = ["common.h", "ops.cuh", "setup.h"]
 
 
@@ -68,6 +71,15 @@ def build(verbose=False, ptxas_info=False):
                 raise subprocess.CalledProcessError(r.returncode, cmd)
     if _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    # the par-file driver, linked against the library with an rpath to it
+    dsrc = [os.path.join(DRIVER, f) for f in DRIVER_SRC]
+    dhdr = [os.path.join(DRIVER, f) for f in ("json.h", "ncclassic.h", "sac.h")] + hdrs
+    if _newer(DRIVER_BIN, dsrc + dhdr + [LIB]):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-o", DRIVER_BIN] + dsrc + \
+              ["-L", LIBDIR, "-lcgfd", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

@@ -297,6 +297,25 @@ int cgfd_setup_dt_max(const cgfd_setup *su, float *d) {
   return CGFD_OK;
 }
 
+int cgfd_select_device(int ordinal) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(CGFD_ERR_NODEVICE, "no CUDA device");
+  if (ordinal < 0 || ordinal >= n) return fail(CGFD_ERR_ARG, "device ordinal out of range");
+  e = cudaSetDevice(ordinal);
+  if (e != cudaSuccess) return cuda_fail(e, "select device");
+  return CGFD_OK;
+}
+
+int cgfd_setup_coords(const cgfd_setup *su, float *x, float *y, float *z) {
+  if (!su) return fail(CGFD_ERR_ARG, "bad argument");
+  const size_t np = su->H.coords.size() / 3;
+  if (x) std::memcpy(x, su->H.coords.data(), np * 4);
+  if (y) std::memcpy(y, su->H.coords.data() + np, np * 4);
+  if (z) std::memcpy(z, su->H.coords.data() + 2 * np, np * 4);
+  return CGFD_OK;
+}
+
 int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes) {
   if (!su || !bytes) return fail(CGFD_ERR_ARG, "bad argument");
   const HostSetup &H = su->H;

@@ -137,6 +137,14 @@ int build_setup(const cgfd_config *c, HostSetup &S, std::string &msg) {
   extrapolate(X.data(), nx, ny, nz, U);
   extrapolate(Y.data(), nx, ny, nz, U);
   extrapolate(Z.data(), nx, ny, nz, U);
+  {
+    const size_t np = (size_t)g.ni * g.nj * g.nk;
+    S.coords.resize(3 * np);
+    for (int k = 0; k < g.nk; k++) for (int j = 0; j < g.nj; j++) for (int i = 0; i < g.ni; i++) {
+      const size_t s = (size_t)i + (size_t)g.ni * ((size_t)j + (size_t)g.nj * k), d = U(i+NG, j+NG, k+NG);
+      S.coords[s] = X[d]; S.coords[np + s] = Y[d]; S.coords[2 * np + s] = Z[d];
+    }
+  }
 
   // ---- metric (gd_curv_metric_cal, gd_t.cu:210-304) ----------------------
   // 6th-order centred differences with the reference's rounded weights

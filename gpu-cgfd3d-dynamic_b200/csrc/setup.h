@@ -36,6 +36,7 @@ struct HostSetup {
   std::vector<float> metric;      // [10][scmp]
   std::vector<float> media;       // [3][scmp]: lambda, mu, 1/rho
   std::vector<float> free_mat;    // [2][ny][nx][9]: matVx2Vz, matVy2Vz at the surface
+  std::vector<float> coords;      // [3][nk][nj][ni]: x, y, z of the interior grid points
   PmlHost pml[3][2];
   std::vector<FaultHost> faults;
   // stations

@@ -27,9 +27,11 @@ MPA = 1.0e6
 
 
 def _homog(ni, nj, nk, vp=6000.0, vs=3464.0, rho=2670.0):
-    # md_gen_uniform_el_iso (src/forward/md_t.cu:378-417)
-    mu = np.float32(vs * vs * rho)
-    lam = np.float32(vp * vp * rho - 2.0 * float(mu))
+    # md_gen_uniform_el_iso (src/forward/md_t.cu:378-417): products in
+    # float, the subtraction of 2 mu in double
+    vp32, vs32, rho32 = np.float32(vp), np.float32(vs), np.float32(rho)
+    mu = vs32 * vs32 * rho32
+    lam = np.float32(float(vp32 * vp32 * rho32) - 2.0 * float(mu))
     shape = (nk, nj, ni)
     return (np.full(shape, lam, np.float32), np.full(shape, mu, np.float32),
             np.full(shape, np.float32(rho), np.float32))

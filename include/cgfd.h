@@ -144,12 +144,20 @@ int cgfd_abi_version(void);
 int cgfd_prepare(const cgfd_config *cfg, cgfd_setup **out);
 /* Bytes that cgfd_upload copies to the device. */
 int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes);
+/* Grid coordinates of a prepared problem, interior points, [nk][nj][ni]
+ * each (any of x, y, z may be NULL): the imported grid, or the grid the
+ * fault-plane extrusion made (gd_curv_gen_fault, gd_t.cu:402-545). */
+int cgfd_setup_coords(const cgfd_setup *su, float *x, float *y, float *z);
 /* Largest stable dt of a prepared problem (CFL 1.3). */
 int cgfd_setup_dt_max(const cgfd_setup *su, float *dtmax);
 /* Device half of cgfd_create: allocate the device state on the current
  * device and copy the prepared problem (drv_rk_curv_col.cu:90-100). */
 int cgfd_upload(const cgfd_setup *su, cgfd_solver **out);
 void cgfd_setup_free(cgfd_setup *su);
+
+/* Make GPU `ordinal` the current device of the calling thread for the
+ * calls that follow (the reference's gpu_id_start argument of main). */
+int cgfd_select_device(int ordinal);
 
 /* Fill cfg with the reference's defaults (welded margin 40, dynamic
  * method 2, stability check on, no PML, free surface off). */
