@@ -707,7 +707,10 @@ __global__ void k_advance(Ctl *c, int max_rec) {
 }
 
 // ---------------------------------------------------------------------------
-int launch_fault_stage(const FaultArgs &a, cudaStream_t st) {
+// first part of a stage: welded nodes, tractions, trial traction and
+// friction (which also refreshes the stage input at i0, read by the volume
+// kernels); returns the number of launches
+int launch_fault_pre(const FaultArgs &a, cudaStream_t st) {
   {
     dim3 blk(32, 4), grd((a.g.nj + 31) / 32, (a.g.nk + 3) / 4);
     k_fault_weld<<<grd, blk, 0, st>>>(a);
@@ -721,6 +724,13 @@ int launch_fault_stage(const FaultArgs &a, cudaStream_t st) {
     dim3 blk(32, 4), grd((a.nj + 31) / 32, (a.nk + 3) / 4);
     k_fault_trial<<<grd, blk, 0, st>>>(a);
   }
+  return 3;
+}
+
+// second part: slab velocity and stress, split nodes; independent of the
+// volume kernels of the same stage (disjoint outputs, shared read-only input)
+int launch_fault_post(const FaultArgs &a, cudaStream_t st) {
+  if (a.nj <= 0 || a.nk <= 0) return 0;
   const long nslab = (long)a.nj * a.nk * 6;
   k_fault_vslab<<<(unsigned)((nslab + 191) / 192), 192, 0, st>>>(a);
   k_fault_sslab<<<(unsigned)((nslab + 191) / 192), 192, 0, st>>>(a);
@@ -728,7 +738,7 @@ int launch_fault_stage(const FaultArgs &a, cudaStream_t st) {
     dim3 blk(32, 4), grd((a.nj + 31) / 32, (a.nk + 3) / 4);
     k_fault_node<<<grd, blk, 0, st>>>(a);
   }
-  return 6;
+  return 3;
 }
 
 void launch_record(const StationArgs &a, cudaStream_t st) {
