@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hills", choices=["hills", "hills_medium", "tpv"])
+    ap.add_argument("--workload", default="hills", choices=["hills", "hills_medium", "tpv", "large"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", type=int, default=0, metavar="N",
                     help="batched form: N seeded scenarios of uneven size advanced as one ensemble, against a "
@@ -57,6 +57,11 @@ def make_problem(workload):
     import inputs
     if workload == "tpv":
         return inputs.tpv_planar(), "tpv_planar 160x100x80 (x strike, y normal, z depth), h=200 m, homogeneous, planar fault"
+    if workload == "large":
+        return (inputs.hills_layered(ni=600, nj=1200, nk=400, h=50.0, pml=20, fault_len=800, fault_depth=360,
+                                     nuc_half=30, dip=25.0, vk_stress=True, nt=4000),
+                "hills_layered 1200x600x400 (x strike, y normal, z depth), h=50 m, 8 hills, 4 layers +3%, "
+                "25-degree dipping fault 800x360 nodes, von Karman shear stress, 20-layer CFS-PML, 32 stations")
     if workload == "hills_medium":
         # the same construction at 300x200x160 (2 GB on the device): the case
         # the ncu captures of the kernels run on

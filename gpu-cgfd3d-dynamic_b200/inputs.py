@@ -113,7 +113,7 @@ def _smooth(a, n):
 
 def hills_layered(ni=300, nj=600, nk=240, h=100.0, pml=20, seed=1001, nsta=32,
                   fault_len=400, fault_depth=180, margin=40, dynamic_method=2, nt=3000,
-                  cfl=0.5, nhills=8):
+                  cfl=0.5, nhills=8, dip=None, vk_stress=False, nuc_half=7):
     """Curvilinear 600x300x240 case (x strike 600, y normal 300, z 240 in the
     task's axes; here ni = 300 normal, nj = 600 strike, nk = 240 up).
 
@@ -122,7 +122,15 @@ def hills_layered(ni=300, nj=600, nk=240, h=100.0, pml=20, seed=1001, nsta=32,
     surface.  Medium: four layers with Vs 2.0/2.6/3.1/3.6 km/s, Vp = 1.73 Vs,
     rho = 310 Vp^0.25 (Gardner), times (1 + 0.03 N(0,1)) smoothed.  Vertical
     fault at the x centre, fault_len x fault_depth nodes below the surface,
-    friction as in ``tpv_planar``; 20-layer PML; dt = cfl * h / (sqrt(3) Vp_max)."""
+    friction as in ``tpv_planar``; 20-layer PML; dt = cfl * h / (sqrt(3) Vp_max).
+
+    ``dip`` (degrees): the grid is sheared along x by depth * cot(dip), so
+    the fault plane i = ni // 2 dips at that angle below the topography
+    (dt then uses the sheared cell's point-to-plane distance
+    h / sqrt(2 + (1 + cot dip)^2)).  ``vk_stress``: the shear traction is a
+    von Karman field (correlation 2 km, Hurst 0.8, std 8 MPa, mean 60 MPa)
+    kept 0.5 MPa below the static strength outside the nucleation patch.
+    With a dip, the 100 MPa compression acts along the plane's normal."""
     rng = np.random.default_rng(seed)
     i0 = ni // 2                         # 0-based fault plane
     xs = (np.arange(ni) - i0) * h
@@ -139,9 +147,12 @@ def hills_layered(ni=300, nj=600, nk=240, h=100.0, pml=20, seed=1001, nsta=32,
     zb = -(nk - 1) * h
     t = np.arange(nk) / (nk - 1.0)
     z3 = zb + (topo[None, :, :] - zb) * t[:, None, None]          # [nk, nj, ni]
-    x3 = np.broadcast_to(X2[None], (nk, nj, ni))
-    y3 = np.broadcast_to(Y2[None], (nk, nj, ni))
     depth = topo[None] - z3
+    if dip is None:
+        x3 = np.broadcast_to(X2[None], (nk, nj, ni))
+    else:
+        x3 = (X2[None] + depth * (1.0 / math.tan(math.radians(dip)))).astype(np.float32)
+    y3 = np.broadcast_to(Y2[None], (nk, nj, ni))
     bounds = [0.0, 2000.0, 6000.0, 12000.0]
     vs_l = [2000.0, 2600.0, 3100.0, 3600.0]
     vs = np.full(depth.shape, vs_l[0])
@@ -155,12 +166,30 @@ def hills_layered(ni=300, nj=600, nk=240, h=100.0, pml=20, seed=1001, nsta=32,
     mu = (vs * vs * rho).astype(np.float32)
     lam = (vp * vp * rho - 2.0 * vs * vs * rho).astype(np.float32)
     vp_max = float(vp.max())
-    dt = cfl * h / (math.sqrt(3.0) * vp_max)
+    del vs, vp, pert
+    if dip is None:
+        dt = cfl * h / (math.sqrt(3.0) * vp_max)
+    else:
+        cot = 1.0 / math.tan(math.radians(dip))
+        dt = cfl * h / (math.sqrt(2.0 + (1.0 + cot) ** 2) * vp_max)
     dt = float(f"{dt:.3g}")
     jc = nj // 2
     fault_grid = [jc - fault_len // 2 + 1, jc + fault_len // 2, nk - fault_depth + 1, nk]
     kc = nk - 1 - fault_depth // 2
-    st = _stress(nj, nk, fault_grid, (jc - 1, kc), 7)
+    ts_field = None
+    if vk_stress:
+        strength = 0.65 * 100.0
+        ts_field = np.minimum(60.0 + 8.0 * von_karman(nj, nk, h, rng=rng), strength - 0.5) * MPA
+    # with a dip, the topography tilts the local normal and the projected
+    # traction: the patch is raised to 80 MPa so that it still nucleates
+    st = _stress(nj, nk, fault_grid, (jc - 1, kc), nuc_half, ts_field=ts_field,
+                 t_nuc=70.0 if dip is None else 80.0)
+    if dip is not None:
+        # compression of 100 MPa along the dipping plane's normal
+        # (sin dip, 0, cos dip); the shear stays along strike (y)
+        d = math.radians(dip)
+        st = (np.full((nk, nj), -100.0 * MPA * math.sin(d), np.float32), st[1],
+              np.full((nk, nj), -100.0 * MPA * math.cos(d), np.float32)) + tuple(st[3:])
     sta = np.stack([rng.integers(pml + 4, ni - pml - 4, nsta), rng.integers(pml + 4, nj - pml - 4, nsta),
                     np.full(nsta, nk - 1)], 1).astype(np.float32)
     fsta = np.array([[jc - 1, kc], [jc - 1 + fault_len // 4, kc], [jc - 1, nk - 1]], np.float32)
@@ -284,3 +313,32 @@ def ensemble_scenarios(n=64, seed=1003, nt=1500, size_lo=(64, 96, 64), size_hi=(
                            fault_stations=np.array([[jc, kc]], np.float32), max_records=nt + 1,
                            name=f"scenario_{q}_{nj}x{ni}x{nk}_{'hills' if hills else 'flat'}", **geo))
     return out
+
+
+def two_faults(nt=60, dynamic_method=2, seed=9):
+    """Two parallel vertical faults 14 nodes apart in a 44x64x32 planar grid
+    (h = 200 m), each with its own fault_grid, nucleation patch and friction:
+    the multi-fault path (one fault_coord / init_stress set per fault)."""
+    ni, nj, nk, h = 44, 64, 32, 200.0
+    lam, mu, rho = _homog(ni, nj, nk)
+    fxi = [15, 29]
+    grids = [[9, 56, 9, 32], [13, 52, 11, 32]]
+    nucs = [((30, 22), 3), ((36, 20), 2)]
+    jj, kk = np.meshgrid(np.arange(1, nj + 1), np.arange(1, nk + 1))
+    fx = np.stack([np.zeros((nk, nj)), np.full((nk, nj), (fxi[1] - fxi[0]) * h)]).astype(np.float32)
+    fy = np.stack([(jj - nj / 2.0) * h] * 2).astype(np.float32)
+    fz = np.stack([(kk - nk) * h] * 2).astype(np.float32)
+    sts = [_stress(nj, nk, g, c, r, mu_s=ms, dc=dc) for g, (c, r), ms, dc in
+           zip(grids, nucs, (0.65, 0.62), (0.30, 0.25))]
+    arr = lambda q: np.stack([st[q] for st in sts])
+    rng = np.random.default_rng(seed)
+    stations = np.stack([rng.integers(7, ni - 7, 4), rng.integers(7, nj - 7, 4), np.full(4, nk - 1)], 1).astype(np.float32)
+    P = ((5, 5), (5, 5), (5, 0))
+    vp = float(np.sqrt((lam[0, 0, 0] + 2 * mu[0, 0, 0]) / rho[0, 0, 0]))
+    return Problem(ni=ni, nj=nj, nk=nk, dt=0.01, lam=lam, mu=mu, rho=rho, fault_x_index=fxi, fault_grid=grids,
+                   T0x=arr(0), T0y=arr(1), T0z=arr(2), mu_s=arr(3), mu_d=arr(4), Dc=arr(5), C0=arr(6),
+                   dynamic_method=dynamic_method, welded_margin=8, free_surface=1, pml_layers=P,
+                   pml_ref_vel=((vp, vp),) * 3, grid_mode=GRID_FAULT_PLANE, fault_interval=h,
+                   fault_x=fx, fault_y=fy, fault_z=fz, stations=stations,
+                   fault_stations=np.array([[30, 22], [36, 20]], np.float32),
+                   fault_station_fault=np.array([0, 1], np.int32), max_records=nt + 1, name="two_faults_64x44x32")

@@ -96,11 +96,13 @@ def _driver():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("medium,hills", [("import", False), ("code", True)])
-def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, hills):
+@pytest.mark.parametrize("medium,case", [("import", "planar"), ("code", "hills"), ("import", "two_faults")])
+def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, case):
     from cgfd import Solver
     nt, skip = 30, 3
-    if hills:
+    if case == "two_faults":
+        p = inputs.two_faults(nt=nt)
+    elif case == "hills":
         p = inputs.hills_layered(ni=48, nj=72, nk=40, h=100.0, pml=8, nsta=4, fault_len=48, fault_depth=30,
                                  margin=6, nt=nt, nhills=2)
         lam, mu, rho = inputs._homog(p.ni, p.nj, p.nk)   # the driver's uniform medium
@@ -111,16 +113,20 @@ def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, hills):
     r = subprocess.run([_driver(), par], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     out = json.load(open(par))["output_dir"]
-    d = par_files.read_fault_output(os.path.join(out, f"fault_i{p.fault_x_index[0]}_px0_py0_pz0.nc"))
-    assert d["Tn"].shape == (nt // skip, p.nk, p.nj)
+    ds = [par_files.read_fault_output(os.path.join(out, f"fault_i{x}_px0_py0_pz0.nc")) for x in p.fault_x_index]
+    for d in ds:
+        assert d["Tn"].shape == (nt // skip, p.nk, p.nj)
     s = Solver(p)
     for rec in range(nt // skip):
-        np.testing.assert_allclose(d["time"][rec], rec * skip * p.dt, rtol=1e-6)
-        for q, f in enumerate(par_files.FAULT_CMP):
-            assert np.array_equal(d[f][rec], s.fault(f)), (rec, f)
+        for fi, d in enumerate(ds):
+            np.testing.assert_allclose(d["time"][rec], rec * skip * p.dt, rtol=1e-6)
+            for q, f in enumerate(par_files.FAULT_CMP):
+                assert np.array_equal(d[f][rec], s.fault(f, fi)), (rec, fi, f)
         s.run(skip)
-    assert np.array_equal(d["Peak_vs"], s.fault("Peak_vs"))
-    assert np.array_equal(d["Init_t0"], s.fault("Init_t0"))
+    for fi, d in enumerate(ds):
+        assert np.array_equal(d["Peak_vs"], s.fault("Peak_vs", fi))
+        assert np.array_equal(d["Init_t0"], s.fault("Init_t0", fi))
+        assert int(np.ravel(d["_attrs"]["i_index_with_ghosts_in_this_thread"])[0]) == p.fault_x_index[fi] + 2
     assert s.fault("Vs").max() > 0.05
     seis = s.stations()
     for q in range(len(p.stations)):

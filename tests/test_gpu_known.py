@@ -112,3 +112,40 @@ def test_tpv_planar_full_600_steps(cgfd_lib, oracle_built):
     assert np.abs(t0s[rup] - t0o[rup]).max() <= p.dt * 1.0001
     assert rel_l2(s.stations()[:, :3], o.stations()[:, :3]) < 1e-4
     assert rel_l2(s.fault_stations(), o.fault_stations()) < 1e-4
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_two_faults(cgfd_lib, oracle_built, method):
+    """Two parallel faults, each with its own fault_grid, stress and friction:
+    both ruptures, the fault stations of each and the wavefield between them."""
+    from oracle import OracleSolver
+    p = inputs.two_faults(dynamic_method=method, nt=60)
+    s, o = Solver(p), OracleSolver(p)
+    s.run(60)
+    o.run(60)
+    for f in range(2):
+        assert o.fault("Vs", f).max() > 0.5
+        for name in ("Vs", "Slip", "Peak_vs", "Tn", "Ts1"):
+            assert rel_l2(s.fault(name, f), o.fault(name, f)) < 1e-4, (f, name)
+        assert np.array_equal(s.fault("Init_t0", f) > 0, o.fault("Init_t0", f) > 0)
+    assert rel_l2(s.fault_stations(), o.fault_stations()) < 1e-4
+    assert rel_l2(s.stations()[:, :3], o.stations()[:, :3]) < 1e-4
+    for c in range(9):
+        assert rel_l2(s.wavefield(c), o.wavefield(c)) < 1e-4, WAVE_COMPONENTS[c]
+
+
+def test_dipping_fault_small(cgfd_lib, oracle_built):
+    """A 25-degree dipping fault meshed into a sheared curvilinear grid under
+    hills, von Karman shear stress: 40 steps against the oracle."""
+    from oracle import OracleSolver
+    p = inputs.hills_layered(ni=64, nj=96, nk=48, h=50.0, pml=8, nsta=4, fault_len=64, fault_depth=36, margin=6,
+                             nt=40, nhills=3, dip=25.0, vk_stress=True, nuc_half=6)
+    s, o = Solver(p), OracleSolver(p)
+    s.run(40)
+    o.run(40)
+    assert o.fault("Vs").max() > 0.5
+    for f in ("Vs", "Slip", "Peak_vs", "Tn", "Ts1", "Ts2"):
+        assert rel_l2(s.fault(f), o.fault(f)) < 1e-4, f
+    assert rel_l2(s.stations()[:, :3], o.stations()[:, :3]) < 1e-4
+    for c in range(9):
+        assert rel_l2(s.wavefield(c), o.wavefield(c)) < 1e-4, WAVE_COMPONENTS[c]
