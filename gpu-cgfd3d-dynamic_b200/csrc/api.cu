@@ -7,7 +7,6 @@
 // sample, 4 x (fault-plane kernels + fused volume kernel) and the step
 // counter advance.  Time levels P and E swap by step parity, which it % 8
 // fixes, so the graphs never need their arguments updated.
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,15 +28,6 @@ void launch_volume_shell(const VolArgs &a, int idir, int jdir, int kdir, int mod
 void launch_volume_face_x(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
-void volume_zq_layout(VolArgs &a, const int box[6], int kchunk);
-cudaError_t volume_sm_prepare();
-void volume_sm_layout(VolArgs &a, const int box[6], int kchunk);
-void launch_volume_sm(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
-void launch_volume_zq(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
-void volume_tma_prepare();
-int volume_tma_encode(CUtensorMap *tm, const float *level, const Grid &g);
-void launch_volume_tma(const CUtensorMap &tm, const VolArgs &a, int idir, int jdir, int kdir, int mode,
-                       cudaStream_t st);
 int launch_fault_pre(const FaultArgs &a, cudaStream_t st);
 int launch_fault_post(const FaultArgs &a, cudaStream_t st);
 cudaError_t noalloc_scratch_address(float **p);
@@ -109,13 +99,9 @@ struct cgfd_solver {
   long long int_points = 0, vol_points = 0;   // points one launch updates
   int it = 0;
   long long launches_per_step = 0, last_launches = 0;
-  int tiled = 0, kchunk = 32;           // volume kernels: 0 boxes, 2 TMA-fed, 3 z-marching interior + boxes
-  int kchunk_zq = 32;
   int ychunk = 16;                      // interior kernel: y tiles per z-marching chunk
   bool pack = true;                     // pack boxes at most 24 points wide (x PML slabs)
-  int kchunk_tma = 32;
   int box_top[1][6];                    // rows under the free surface
-  CUtensorMap tmap[4];                  // TMA maps of the 4 level slots
   int box_in[1][6];                     // interior box (no PML, no surface rows)
   // boxes of each volume kernel kind: 0 interior, 1 generic shell (PML
   // edges / corners, surface rows), 2..4 slabs reached by the PML faces of
@@ -230,36 +216,9 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       v.pml[q].aout = sout >= 0 ? s->pml[q].aux[sout] : nullptr; v.pml[q].aend = s->pml[q].aux[send];
     }
     VolArgs vs = v;
-    v.kchunk = s->kchunk;
-    v.ctl_err = &s->ctl->err;
-    if (s->tiled == 2) {
-      // rows under the free surface go to the box kernel (traction image,
-      // velocity-low operators), everything below to the TMA kernel
-      v.kend = s->isfree ? s->g.nk - 4 : s->g.nk;
-      v.kchunk = s->kchunk_tma;
-      launch_volume_tma(s->tmap[scur], v, idir, jdir, kdir, mode, s->stream);
-      volume_boxes(vs, s->box_top, 1, true);
-      launch_volume_shell(vs, idir, jdir, kdir, mode, s->stream);
-      nl += 1 + (vs.nbox > 0);
-    } else {
-      // interior box (z-marching kernel when selected), single-direction
-      // PML slabs, generic shell
-      int kind0 = 0;
-      if (s->tiled == 3) {
-        VolArgs vz = v;
-        volume_zq_layout(vz, s->box_in[0], s->kchunk_zq);
-        launch_volume_zq(vz, idir, jdir, kdir, mode, s->stream);
-        nl += vz.nbox > 0;
-        kind0 = 1;
-      } else if (s->tiled == 4) {
-        VolArgs vz = v;
-        volume_sm_layout(vz, s->box_in[0], s->kchunk_zq);
-        if (tm) cudaEventRecordWithFlags(s->ev_int0[ip][stage], s->stream, cudaEventRecordExternal);
-        launch_volume_sm(vz, idir, jdir, kdir, mode, s->stream);
-        if (tm) cudaEventRecordWithFlags(s->ev_int[ip][stage], s->stream, cudaEventRecordExternal);
-        nl += vz.nbox > 0;
-        kind0 = 1;
-      }
+    {
+      // interior box, single-direction PML slabs, generic shell
+      const int kind0 = 0;
       for (int kind = kind0; kind < 5; kind++) {
         VolArgs vk = vs;
         volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind != 0 && s->pack);
@@ -397,29 +356,10 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   s->g = H.g; s->imethod = H.imethod; s->isfree = H.isfree; s->dt = H.dt; s->dtmax = H.dtmax;
   const char *ng = std::getenv("CGFD_NO_GRAPH");
   s->use_graph = !(ng && ng[0] == '1');
-  const char *vk = std::getenv("CGFD_VOLUME");
-  s->tiled = 0;
-  if (vk && std::strcmp(vk, "tma") == 0) s->tiled = 2;
-  if (vk && std::strcmp(vk, "zq") == 0) s->tiled = 3;
-  if (vk && std::strcmp(vk, "sm") == 0) s->tiled = 4;
-  {
-    // z chunk per block: enough blocks for several waves, rows >= 8
-    const long bxy = (long)((H.g.ni + 31) / 32) * ((H.g.nj + 7) / 8);
-    const long nch = std::max<long>(1, (2400 + bxy - 1) / bxy);
-    s->kchunk = (int)std::min<long>(64, std::max<long>(8, (H.g.nk + nch - 1) / nch));
-    const int nkt = H.isfree ? H.g.nk - 4 : H.g.nk;
-    s->kchunk_tma = (int)std::min<long>(64, std::max<long>(10, (nkt + nch - 1) / nch));
-  }
   const Grid &g = s->g;
   const size_t lev = (size_t)NCMP * g.scmp, ns = (size_t)g.ny * g.nz;
 #define CK(x, what) do { cudaError_t _e = (x); if (_e != cudaSuccess) { destroy(s); return cuda_fail(_e, what); } } while (0)
   for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
-  if (s->tiled == 4) CK(volume_sm_prepare(), "shared-memory attribute");
-  if (s->tiled == 2) {
-    volume_tma_prepare();
-    for (int L = 0; L < 4; L++)
-      if (volume_tma_encode(&s->tmap[L], s->w[L], g) != 0) { destroy(s); return fail(CGFD_ERR_CUDA, "tensor map encoding failed"); }
-  }
   CK(dalloc(s, &s->met, H.metric.size()), "metric");
   CK(dalloc(s, &s->med, H.media.size()), "medium");
   CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
@@ -532,22 +472,11 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     }
     const int bt[6] = { 0, g.ni - 1, 0, g.nj - 1, s->isfree ? g.nk - 4 : g.nk, g.nk - 1 };
     std::memcpy(s->box_top[0], bt, sizeof bt);
-    // z chunk of the z-marching kernel: about 8 waves of 2 blocks per SM
-    // over the interior box's 32 x 8 tiles, at least 16 rows per chunk
-    int nsm = 148;
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const long tiles = (long)((ihi - ilo + 32) / 32) * ((jhi - jlo + 8) / 8);
-    const long nz = std::max(1, khi - klo + 1);
-    const long nch = std::max<long>(1, (8L * 2 * nsm + tiles - 1) / std::max<long>(1, tiles));
-    s->kchunk_zq = (int)std::max<long>(16, (nz + nch - 1) / nch);
     const char *pk = std::getenv("CGFD_PACK");
     if (pk && pk[0] == '0') s->pack = false;
     const char *yc = std::getenv("CGFD_INTERIOR_YCHUNK");
     if (yc && std::atoi(yc) > 0) s->ychunk = std::atoi(yc);
     s->ychunk = std::min(s->ychunk, std::max(1, (jhi - jlo + 8) / 8));
-    const char *kc = std::getenv("CGFD_ZQ_KCHUNK");
-    if (kc && std::atoi(kc) > 0) s->kchunk_zq = std::atoi(kc);
     // points one interior launch / one volume stage updates: the split-node
     // slabs belong to the fault kernels
     long long nint = (long long)std::max(0, ihi - ilo + 1) * std::max(0, jhi - jlo + 1) * std::max(0, khi - klo + 1);
@@ -595,7 +524,7 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   long long nl = 0;
   double vol_ms = 0, int_ms = 0;
   long long vol_n = 0, int_n = 0;
-  const bool int_timed = (s->tiled == 0 || s->tiled == 4) && s->nkbox[0] > 0;
+  const bool int_timed = s->nkbox[0] > 0;
   // with timing on, the events of step it (recorded by the graph of it % 8)
   // are read just before that graph is launched again 8 steps later, and
   // the last 8 after the loop: the host never waits on the step in flight
@@ -673,7 +602,6 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read control block");
   if (c.it != s->it) return fail(CGFD_ERR_STATE, "device step counter out of step with the host");
-  if (c.err & CTL_ERR_TMA) return fail(CGFD_ERR_CUDA, "volume kernel: a TMA row load did not complete in time");
   if (c.err & CTL_ERR_NONFINITE) return fail(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
   return CGFD_OK;
 }
@@ -738,7 +666,6 @@ int cgfd_run_noalloc(cgfd_solver *s, int nsteps) {
   e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: read control block");
   if (c.it != s->it) return fail_fixed(CGFD_ERR_STATE, "device step counter out of step with the host");
-  if (c.err & CTL_ERR_TMA) return fail_fixed(CGFD_ERR_CUDA, "volume kernel: a TMA row load did not complete in time");
   if (c.err & CTL_ERR_NONFINITE) return fail_fixed(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
   return CGFD_OK;
 }
@@ -829,7 +756,6 @@ int cgfd_ensemble_run(cgfd_ensemble *e, int nsteps) {
     if (er != cudaSuccess) return cuda_fail(er, "read control block");
     const std::string who = "ensemble member " + std::to_string(q) + ": ";
     if (c.it != s->it) return fail(CGFD_ERR_STATE, who + "device step counter out of step with the host");
-    if (c.err & CTL_ERR_TMA) return fail(CGFD_ERR_CUDA, who + "volume kernel: a TMA row load did not complete in time");
     if (c.err & CTL_ERR_NONFINITE) return fail(CGFD_ERR_UNSTABLE, who + "non-finite slip rate or station value");
   }
   return CGFD_OK;

@@ -114,6 +114,6 @@ struct Ctl {
   int err;                  // CTL_ERR_* bits
   int pad;
 };
-enum CtlErr { CTL_ERR_NONFINITE = 1, CTL_ERR_TMA = 2 };
+enum CtlErr { CTL_ERR_NONFINITE = 1 };
 
 }  // namespace cgfd

@@ -69,9 +69,6 @@ struct VolBox {
 
 struct VolArgs {
   Grid g;
-  int kchunk;                  // z rows marched by one block (tiled kernels)
-  int kend;                    // rows [0, kend) handled by the TMA kernel
-  int *ctl_err;                // Ctl::err of the solver
   int nbox, nblocks;
   int ychunk;                  // interior kernel: y tiles per chunk (z marches within a chunk)
   VolBox box[12];
