@@ -849,28 +849,49 @@ int cgfd_get_fault_stations(cgfd_solver *s, float *out, int *nrec) {
   return get_series(s, s->fseis, s->st.nf, out, nrec);
 }
 
+// the array of one level that holds component cmp: the 16-byte groups
+// (Vx Vy Vz Txx), (Tyy Tzz Tyz Txz) or Txy; element of point p at
+// p * step + lane
+struct CmpArray { size_t off, n; int step, lane; };
+static CmpArray cmp_array(const Grid &g, int cmp) {
+  const size_t sc = g.scmp;
+  if (cmp < 4) return { 0, 4 * sc, 4, cmp };
+  if (cmp < 8) return { 4 * sc, 4 * sc, 4, cmp - 4 };
+  return { 8 * sc, sc, 1, 0 };
+}
+
 int cgfd_get_wavefield(cgfd_solver *s, int cmp, float *out) {
   if (!s || !out || cmp < 0 || cmp >= NCMP) return fail(CGFD_ERR_ARG, "bad argument");
   const Grid &g = s->g;
-  std::vector<float> h(g.scmp);
-  cudaError_t e = cudaMemcpyAsync(h.data(), s->w[slot(LP, s->it)] + (size_t)cmp * g.scmp, g.scmp * 4, cudaMemcpyDeviceToHost, s->stream);
+  const CmpArray A = cmp_array(g, cmp);
+  std::vector<float> h(A.n);
+  cudaError_t e = cudaMemcpyAsync(h.data(), s->w[slot(LP, s->it)] + A.off, A.n * 4, cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read wavefield");
-  for (int k = 0; k < g.nk; k++) for (int j = 0; j < g.nj; j++)
-    std::memcpy(out + ((size_t)k * g.nj + j) * g.ni, h.data() + g.at(NG, j + NG, k + NG), (size_t)g.ni * 4);
+  for (int k = 0; k < g.nk; k++)
+    for (int j = 0; j < g.nj; j++) {
+      const float *src = h.data() + (size_t)g.at(NG, j + NG, k + NG) * A.step + A.lane;
+      float *dst = out + ((size_t)k * g.nj + j) * g.ni;
+      for (int i = 0; i < g.ni; i++) dst[i] = src[(size_t)i * A.step];
+    }
   return CGFD_OK;
 }
 
 int cgfd_set_wavefield(cgfd_solver *s, int cmp, const float *in) {
   if (!s || !in || cmp < 0 || cmp >= NCMP) return fail(CGFD_ERR_ARG, "bad argument");
   const Grid &g = s->g;
-  std::vector<float> h(g.scmp);
-  float *dst = s->w[slot(LP, s->it)] + (size_t)cmp * g.scmp;
-  cudaError_t e = cudaMemcpy(h.data(), dst, g.scmp * 4, cudaMemcpyDeviceToHost);
+  const CmpArray A = cmp_array(g, cmp);
+  std::vector<float> h(A.n);
+  float *dst = s->w[slot(LP, s->it)] + A.off;
+  cudaError_t e = cudaMemcpy(h.data(), dst, A.n * 4, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read wavefield");
-  for (int k = 0; k < g.nk; k++) for (int j = 0; j < g.nj; j++)
-    std::memcpy(h.data() + g.at(NG, j + NG, k + NG), in + ((size_t)k * g.nj + j) * g.ni, (size_t)g.ni * 4);
-  e = cudaMemcpy(dst, h.data(), g.scmp * 4, cudaMemcpyHostToDevice);
+  for (int k = 0; k < g.nk; k++)
+    for (int j = 0; j < g.nj; j++) {
+      float *d = h.data() + (size_t)g.at(NG, j + NG, k + NG) * A.step + A.lane;
+      const float *src = in + ((size_t)k * g.nj + j) * g.ni;
+      for (int i = 0; i < g.ni; i++) d[(size_t)i * A.step] = src[i];
+    }
+  e = cudaMemcpy(dst, h.data(), A.n * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "write wavefield");
   return CGFD_OK;
 }

@@ -6,8 +6,10 @@
 // points per side, x fastest, src/forward/gd_t.cu:2124-2140) but with a
 // padded row pitch: index p = (i + XOFF) + j*sy + k*sz for ghost-inclusive
 // indices (i, j, k), sy a multiple of 32 floats.  XOFF = 1 puts the first
-// interior point (i = 3) on a 16-byte boundary.  A wavefield level is 9
-// components of scmp floats (Vx,Vy,Vz,Txx,Tyy,Tzz,Tyz,Txz,Txy); four levels
+// interior point (i = 3) on a 16-byte boundary.  A wavefield level holds the
+// 9 components (Vx,Vy,Vz,Txx,Tyy,Tzz,Tyz,Txz,Txy) of scmp points as two
+// arrays of 16-byte groups (Vx Vy Vz Txx | Tyy Tzz Tyz Txz) and one of Txy,
+// so that a stencil tap reads all nine with three loads (Grid::w); four levels
 // P (time n), A and B (ping-pong stage inputs) and E (time n+1 accumulator)
 // replace the reference's pre/tmp/rhs/end, because each fused stage writes
 // its output level directly instead of a separate rhs array.
@@ -70,7 +72,13 @@ struct Grid {
   long sy, sz;           // strides of j and k (elements)
   long scmp;             // elements per component (sz * nz)
   CGFD_HD long at(int i, int j, int k) const { return (long)(i + XOFF) + (long)j * sy + (long)k * sz; }
+  // element of component c at point p within one wavefield level: the
+  // components 0-3 (Vx Vy Vz Txx) and 4-7 (Tyy Tzz Tyz Txz) are interleaved
+  // in 16-byte groups, Txy is stored alone
+  CGFD_HD long w(int c, long p) const { return c < 4 ? 4 * p + c : (c < 8 ? 4 * scmp + 4 * p + (c - 4) : 8 * scmp + p); }
 };
+// distance between neighbouring points of one wavefield component (floats)
+CGFD_HD constexpr int wstep(int c) { return c < 8 ? 4 : 1; }
 
 struct PmlFaceDev {
   int on, d, s, L;

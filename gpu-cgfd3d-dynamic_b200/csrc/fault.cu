@@ -48,12 +48,15 @@ namespace {
 __device__ __forceinline__ long fidx(int c, int m, long ns, long nd) { return ((long)c * 2 + m) * ns + nd; }
 
 // J * (e_ax . sigma) at point q, 3 components
-__device__ __forceinline__ void trac3(const float *__restrict__ w, const float *__restrict__ met, long sc,
+__device__ __forceinline__ void trac3(const Grid &g, const float *__restrict__ w, const float *__restrict__ met,
                                       long q, int ax, float t[3]) {
+  const long sc = g.scmp;
   const float J = __ldg(met + MJAC * sc + q);
   const float ex = __ldg(met + ax * sc + q), ey = __ldg(met + (ax + 1) * sc + q), ez = __ldg(met + (ax + 2) * sc + q);
-  const float sxx = __ldg(w + TXX * sc + q), syy = __ldg(w + TYY * sc + q), szz = __ldg(w + TZZ * sc + q);
-  const float syz = __ldg(w + TYZ * sc + q), sxz = __ldg(w + TXZ * sc + q), sxy = __ldg(w + TXY * sc + q);
+  // Txx ends the first 16-byte group, Tyy Tzz Tyz Txz are the second
+  const float sxx = __ldg(w + g.w(TXX, q));
+  const float4 s4 = __ldg(reinterpret_cast<const float4 *>(w + 4 * sc) + q);
+  const float syy = s4.x, szz = s4.y, syz = s4.z, sxz = s4.w, sxy = __ldg(w + g.w(TXY, q));
   t[0] = J * (ex * sxx + ey * sxy + ez * sxz);
   t[1] = J * (ex * sxy + ey * syy + ez * syz);
   t[2] = J * (ex * sxz + ey * syz + ez * szz);
@@ -119,17 +122,15 @@ __device__ void split_to_volume(const Grid &g, const float *__restrict__ met, lo
   for (int r = 0; r < 3; r++)
 #pragma unroll
     for (int c = 0; c < 3; c++) st[r][c] = (tr[r][0] * mi[0][c] + tr[r][1] * mi[1][c] + tr[r][2] * mi[2][c]) * rj;
+  float u[3];
 #pragma unroll
-  for (int c = 0; c < 3; c++)
-    wt[(VX + c) * sc + p0] = (f[fidx(FVX + c, 0, ns, nd)] + f[fidx(FVX + c, 1, ns, nd)]) * 0.5f;
-  wt[TXX * sc + p0] = st[0][0];
-  wt[TYY * sc + p0] = st[1][1];
-  wt[TZZ * sc + p0] = st[2][2];
-  wt[TXY * sc + p0] = (st[0][1] + st[1][0]) * 0.5f;
+  for (int c = 0; c < 3; c++) u[c] = (f[fidx(FVX + c, 0, ns, nd)] + f[fidx(FVX + c, 1, ns, nd)]) * 0.5f;
+  reinterpret_cast<float4 *>(wt)[p0] = make_float4(u[0], u[1], u[2], st[0][0]);
   // the reference's fault2wave_gpu receives Tyz and Txz in swapped
   // positions (transform.cu:281-289 vs :293-300); kept for parity
-  wt[TYZ * sc + p0] = (st[0][2] + st[2][0]) * 0.5f;
-  wt[TXZ * sc + p0] = (st[1][2] + st[2][1]) * 0.5f;
+  reinterpret_cast<float4 *>(wt + 4 * sc)[p0] =
+      make_float4(st[1][1], st[2][2], (st[0][2] + st[2][0]) * 0.5f, (st[1][2] + st[2][1]) * 0.5f);
+  wt[g.w(TXY, p0)] = (st[0][1] + st[1][0]) * 0.5f;
 }
 
 }  // namespace
@@ -141,19 +142,19 @@ __global__ void k_fault_weld(const FaultArgs a) {
   const int k = blockIdx.y * blockDim.y + threadIdx.y;
   if (j >= g.nj || k >= g.nk) return;
   const int J = j + NG, K = k + NG;
-  const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny, sc = g.scmp;
+  const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny;
   if (a.F.flag[nd] & FL_SPLIT) return;
   const long p = g.at(a.F.i0, J, K);
   const float *w = a.wcur;
   float t2[3], t3[3];
-  trac3(w, a.met, sc, p, METX, t2);
-  trac3(w, a.met, sc, p, MZTX, t3);
+  trac3(g, w, a.met, p, METX, t2);
+  trac3(g, w, a.met, p, MZTX, t3);
   float *f = const_cast<float *>(a.fc);
 #pragma unroll
   for (int m = 0; m < 2; m++) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      f[fidx(FVX + c, m, ns, nd)] = w[(VX + c) * sc + p];
+      f[fidx(FVX + c, m, ns, nd)] = w[g.w(VX + c, p)];
       f[fidx(FT2X + c, m, ns, nd)] = t2[c];
       f[fidx(FT3X + c, m, ns, nd)] = t3[c];
     }
@@ -175,16 +176,16 @@ __global__ void __launch_bounds__(192) k_fault_trac(const FaultArgs a) {
   const int slot = (int)(t - node * 12);
   const int d = slot < 6 ? slot - 6 : slot - 5;
   const int kk = (int)(node / a.tnj), jj = (int)(node - (long)kk * a.tnj);
-  const long sc = g.scmp, pl = (long)a.tnj * a.tnk * 12;
+  const long pl = (long)a.tnj * a.tnk * 12;
   const long q = g.at(a.F.i0 + d, a.tj0 + jj, a.tk0 + kk);
   float *tp = a.trac + node * 12 + slot;
   float v[3];
-  trac3(a.wcur, a.met, sc, q, MXIX, v);
+  trac3(g, a.wcur, a.met, q, MXIX, v);
   tp[0] = v[0]; tp[pl] = v[1]; tp[2 * pl] = v[2];
   if (d >= -3 && d <= 3) {
-    trac3(a.wcur, a.met, sc, q, METX, v);
+    trac3(g, a.wcur, a.met, q, METX, v);
     tp[3 * pl] = v[0]; tp[4 * pl] = v[1]; tp[5 * pl] = v[2];
-    trac3(a.wcur, a.met, sc, q, MZTX, v);
+    trac3(g, a.wcur, a.met, q, MZTX, v);
     tp[6 * pl] = v[0]; tp[7 * pl] = v[1]; tp[8 * pl] = v[2];
   }
 }
@@ -410,7 +411,7 @@ __global__ void __launch_bounds__(192) k_fault_vslab(const FaultArgs a) {
       for (int l = nf + 1; l < 7; l++) z[l] = -z[2 * nf - l];
     }
     h[c] = (hv[c] + drp_v(y + 3, a.jdir) + drp_v(z + 3, a.kdir)) * rr;
-    o[c] = (VX + c) * sc + q;
+    o[c] = g.w(VX + c, q);
   }
   rk_put_n<3>(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, o, h);
 }
@@ -430,7 +431,8 @@ __global__ void __launch_bounds__(192) k_fault_sslab(const FaultArgs a) {
   if (!(F.flag[nd] & FL_SPLIT)) return;
   const int i0 = F.i0;
   const float *w = a.wcur, *met = a.met;
-  const long sy = g.sy, sz = g.sz;
+  // velocity components sit 4 floats apart from one point to the next
+  const long sy = 4 * g.sy, sz = 4 * g.sz;
   const int km = g.nk - (k + 1);
   const bool fwd = a.idir == 1;
   const bool top = a.isfree && km == 0;
@@ -443,23 +445,23 @@ __global__ void __launch_bounds__(192) k_fault_sslab(const FaultArgs a) {
   float dx[3], dy[3], dz[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const float *v = w + (VX + c) * sc + q;
+    const float *v = w + g.w(VX + c, q);
     const float f = fV[c];
     if (fwd) {
       // forward operators; points left of the fault see the minus side
-      if (s == 3) dx[c] = drp<1>(v, 1);
-      else if (s == 2) dx[c] = mac24(v, 1, 1);
-      else if (s == 1) dx[c] = mac22(v, 1, 1);
+      if (s == 3) dx[c] = drp<1>(v, 4);
+      else if (s == 2) dx[c] = mac24(v, 4, 1);
+      else if (s == 1) dx[c] = mac22(v, 4, 1);
       else if (s == -1) dx[c] = f - __ldg(v);
-      else if (s == -2) dx[c] = kB1 * __ldg(v) + kB2 * __ldg(v + 1) + kB3 * f;
-      else dx[c] = kC1 * __ldg(v - 1) + kC2 * __ldg(v) + kC3 * __ldg(v + 1) + kC4 * __ldg(v + 2) + kC5 * f;
+      else if (s == -2) dx[c] = kB1 * __ldg(v) + kB2 * __ldg(v + 4) + kB3 * f;
+      else dx[c] = kC1 * __ldg(v - 4) + kC2 * __ldg(v) + kC3 * __ldg(v + 4) + kC4 * __ldg(v + 8) + kC5 * f;
     } else {
-      if (s == -3) dx[c] = drp<0>(v, 1);
-      else if (s == -2) dx[c] = mac24(v, 1, 0);
-      else if (s == -1) dx[c] = mac22(v, 1, 0);
+      if (s == -3) dx[c] = drp<0>(v, 4);
+      else if (s == -2) dx[c] = mac24(v, 4, 0);
+      else if (s == -1) dx[c] = mac22(v, 4, 0);
       else if (s == 1) dx[c] = __ldg(v) - f;
-      else if (s == 2) dx[c] = -(kB3 * f + kB2 * __ldg(v - 1) + kB1 * __ldg(v));
-      else dx[c] = -(kC5 * f + kC4 * __ldg(v - 2) + kC3 * __ldg(v - 1) + kC2 * __ldg(v) + kC1 * __ldg(v + 1));
+      else if (s == 2) dx[c] = -(kB3 * f + kB2 * __ldg(v - 4) + kB1 * __ldg(v));
+      else dx[c] = -(kC5 * f + kC4 * __ldg(v - 8) + kC3 * __ldg(v - 4) + kC2 * __ldg(v) + kC1 * __ldg(v + 4));
     }
     dy[c] = drp_rt(v, sy, a.jdir);
     if (a.isfree && km == 1) dz[c] = mac22(v, sz, a.kdir);
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(192) k_fault_sslab(const FaultArgs a) {
   h[5] = mu * (G[0][1] + G[1][0]);   // Txy
   long o[6];
 #pragma unroll
-  for (int c = 0; c < 6; c++) o[c] = (TXX + c) * sc + q;
+  for (int c = 0; c < 6; c++) o[c] = g.w(TXX + c, q);
   rk_put_n<6>(a.mode, a.ca, a.cb, a.wcur, a.wpre, a.wout, a.wend, o, h);
 }
 
@@ -548,7 +550,7 @@ __global__ void __launch_bounds__(128) k_fault_node(const FaultArgs a) {
       if (fwd) {
         const long q = g.at(i0 + 1, J, K);
 #pragma unroll
-        for (int c = 0; c < 3; c++) Sx[1][c] = w[(VX + c) * sc + q] - fV[1][c];
+        for (int c = 0; c < 3; c++) Sx[1][c] = w[g.w(VX + c, q)] - fV[1][c];
         mv3(M(FM_P2M1), Sx[1], o1); mv3(M(FM_P2M2), Sy[1], o2); mv3(M(FM_P2M3), Sz[1], o3);
         mv3(M(FM_P2M4), Sy[0], o4); mv3(M(FM_P2M5), Sz[0], o5);
 #pragma unroll
@@ -556,7 +558,7 @@ __global__ void __launch_bounds__(128) k_fault_node(const FaultArgs a) {
       } else {
         const long q = g.at(i0 - 1, J, K);
 #pragma unroll
-        for (int c = 0; c < 3; c++) Sx[0][c] = fV[0][c] - w[(VX + c) * sc + q];
+        for (int c = 0; c < 3; c++) Sx[0][c] = fV[0][c] - w[g.w(VX + c, q)];
         mv3(M(FM_M2P1), Sx[0], o1); mv3(M(FM_M2P2), Sy[0], o2); mv3(M(FM_M2P3), Sz[0], o3);
         mv3(M(FM_M2P4), Sy[1], o4); mv3(M(FM_M2P5), Sz[1], o5);
 #pragma unroll
@@ -582,14 +584,14 @@ __global__ void __launch_bounds__(128) k_fault_node(const FaultArgs a) {
       if (fwd) {
         const long q = g.at(i0 + 1, J, K);
 #pragma unroll
-        for (int c = 0; c < 3; c++) Sx[1][c] = w[(VX + c) * sc + q] - fV[1][c];
+        for (int c = 0; c < 3; c++) Sx[1][c] = w[g.w(VX + c, q)] - fV[1][c];
         mv3(FM(FF_P2M1), Sx[1], o1); mv3(FM(FF_P2M2), Sy[1], o2); mv3(FM(FF_P2M3), Sy[0], o3);
 #pragma unroll
         for (int c = 0; c < 3; c++) Sx[0][c] = o1[c] + o2[c] - o3[c];
       } else {
         const long q = g.at(i0 - 1, J, K);
 #pragma unroll
-        for (int c = 0; c < 3; c++) Sx[0][c] = fV[0][c] - w[(VX + c) * sc + q];
+        for (int c = 0; c < 3; c++) Sx[0][c] = fV[0][c] - w[g.w(VX + c, q)];
         mv3(FM(FF_M2P1), Sx[0], o1); mv3(FM(FF_M2P2), Sy[0], o2); mv3(FM(FF_M2P3), Sy[1], o3);
 #pragma unroll
         for (int c = 0; c < 3; c++) Sx[1][c] = o1[c] + o2[c] - o3[c];
@@ -682,10 +684,15 @@ __global__ void k_record(const StationArgs a) {
   if (rec >= S.max_rec) return;
   if (t < S.n * 9) {
     const int n = t / 9, c = t % 9;
-    const long *ix = S.idx + (long)n * 8;
+    const long *ixp = S.idx + (long)n * 8;
     const float Lx2 = S.w[3 * n], Ly2 = S.w[3 * n + 1], Lz2 = S.w[3 * n + 2];
     const float Lx1 = 1.0f - Lx2, Ly1 = 1.0f - Ly2, Lz1 = 1.0f - Lz2;
-    const float *v = a.w + (long)c * a.g.scmp;
+    // component c of the level: points 4 floats apart in the grouped
+    // arrays, 1 float apart for Txy
+    const float *v = a.w + a.g.w(c, 0);
+    const int u4 = wstep(c);
+    const long ix[8] = { u4 * ixp[0], u4 * ixp[1], u4 * ixp[2], u4 * ixp[3],
+                         u4 * ixp[4], u4 * ixp[5], u4 * ixp[6], u4 * ixp[7] };
     const float b0 = v[ix[0]], b1 = v[ix[1]], b2 = v[ix[2]], b3 = v[ix[3]];
     const float b5 = v[ix[5]], b6 = v[ix[6]], b7 = v[ix[7]];
     const float r = b0 * Lx1 * Ly1 * Lz1 + b1 * Lx2 * Ly1 * Lz1 + b2 * Lx1 * Ly2 * Lz1 + b3 * Lx2 * Ly2 * Lz1 +

@@ -20,11 +20,12 @@
 // the input level (stencil taps come from L1/L2), the metric and the medium
 // once and writes the output levels once.
 //
-// Each component's taps are addressed from one base pointer: x taps are
-// immediate offsets, y / z taps share two int offset tables, the centre
-// sample is loaded once for all three directions.  The RHS is built
-// direction by direction, so a PML face of normal d reuses direction d's
-// contribution.
+// A level stores the nine components of a point in two 16-byte groups and
+// one float (Grid::w), so a stencil tap is three loads: x taps are
+// immediate offsets from three base pointers, y / z taps share two int
+// offset tables, the centre sample is loaded once for all three
+// directions.  The RHS is built direction by direction, so a PML face of
+// normal d reuses direction d's contribution.
 //
 // Roofline: HBM-bound.  Algorithmic traffic per point and step is
 // 192 floats = 768 B (21+18, 39+18, 39+18, 30+9 floats over the 4 stages).
@@ -42,14 +43,36 @@ constexpr int BX = 32, BY = 8;
 // conservative traction J * (e . sigma_row) at point q for metric row `ax`
 // (MXIX, METX or MZTX) and stress row r (0: xx,xy,xz; 1: xy,yy,yz;
 // 2: xz,yz,zz)
-__device__ __forceinline__ float ctrac(const float *__restrict__ w, const float *__restrict__ met,
-                                       long sc, long q, int ax, int r) {
+__device__ __forceinline__ float ctrac(const Grid &g, const float *__restrict__ w, const float *__restrict__ met,
+                                       long q, int ax, int r) {
+  const long sc = g.scmp;
   const int c0 = r == 0 ? TXX : (r == 1 ? TXY : TXZ);
   const int c1 = r == 0 ? TXY : (r == 1 ? TYY : TYZ);
   const int c2 = r == 0 ? TXZ : (r == 1 ? TYZ : TZZ);
-  return __ldg(met + MJAC * sc + q) * (__ldg(met + ax * sc + q) * __ldg(w + c0 * sc + q) +
-                                       __ldg(met + (ax + 1) * sc + q) * __ldg(w + c1 * sc + q) +
-                                       __ldg(met + (ax + 2) * sc + q) * __ldg(w + c2 * sc + q));
+  return __ldg(met + MJAC * sc + q) * (__ldg(met + ax * sc + q) * __ldg(w + g.w(c0, q)) +
+                                       __ldg(met + (ax + 1) * sc + q) * __ldg(w + g.w(c1, q)) +
+                                       __ldg(met + (ax + 2) * sc + q) * __ldg(w + g.w(c2, q)));
+}
+
+// the point's three groups within one level
+struct Taps {
+  const float4 *__restrict__ a;  // Vx Vy Vz Txx
+  const float4 *__restrict__ b;  // Tyy Tzz Tyz Txz
+  const float *__restrict__ t;   // Txy
+};
+__device__ __forceinline__ Taps taps_at(const float *w, long sc, long p) {
+  Taps T;
+  T.a = reinterpret_cast<const float4 *>(w) + p;
+  T.b = reinterpret_cast<const float4 *>(w + 4 * sc) + p;
+  T.t = w + 8 * sc + p;
+  return T;
+}
+// the nine components of the point o points away
+__device__ __forceinline__ void ld9(const Taps &T, int o, float v[9]) {
+  const float4 x = __ldg(T.a + o), y = __ldg(T.b + o);
+  v[VX] = x.x; v[VY] = x.y; v[VZ] = x.z; v[TXX] = x.w;
+  v[TYY] = y.x; v[TZZ] = y.y; v[TYZ] = y.z; v[TXZ] = y.w;
+  v[TXY] = __ldg(T.t + o);
 }
 
 template <int F>
@@ -58,18 +81,6 @@ __device__ __forceinline__ float wdrp(int n) {
            : (n == 0 ? -kC5 : n == 1 ? -kC4 : n == 2 ? -kC3 : n == 3 ? -kC2 : -kC1);
 }
 
-// one-sided DRP derivative of the component at wc with the centre sample v0
-// known; off[n] are the offsets of the 4 other taps in table order
-template <int F>
-__device__ __forceinline__ float drp_c(const float *__restrict__ wc, float v0, const int off[4]) {
-  // table order: F: -1, 0, 1, 2, 3; B: -3, -2, -1, 0, 1 (centre at n = 1 / 3)
-  if (F)
-    return kC1 * __ldg(wc + off[0]) + kC2 * v0 + kC3 * __ldg(wc + off[1]) + kC4 * __ldg(wc + off[2]) +
-           kC5 * __ldg(wc + off[3]);
-  else
-    return -(kC5 * __ldg(wc + off[0]) + kC4 * __ldg(wc + off[1]) + kC3 * __ldg(wc + off[2]) + kC2 * v0 +
-             kC1 * __ldg(wc + off[3]));
-}
 template <int F>
 __device__ __forceinline__ void tap_offsets(int s, int off[4]) {
   if (F) { off[0] = -s; off[1] = s; off[2] = 2 * s; off[3] = 3 * s; }
@@ -90,31 +101,55 @@ __device__ __forceinline__ void rhs_dir(const float D[9], const float e[3], floa
   r[TYZ] = mu * (e[2] * D[VY] + e[1] * D[VZ]);
 }
 
-// Accumulate one direction's derivatives straight into the velocity
-// gradient G[c][b] = dV_c/dx_b and the momentum sums
-// s_r = sum_a e_a . d(sigma_row r)/dxi_a (12 live accumulators).
+// one-sided DRP derivatives of the nine components, the centre sample v0
+// known; off[n] are the offsets of the 4 other taps in table order
+// (F: -1, 0, 1, 2, 3; B: -3, -2, -1, 0, 1 with the centre at n = 1 / 3).
+// Each tap's nine components come in one go; the sums keep the order of
+// the coefficient table.
 template <int F>
-__device__ __forceinline__ void acc_dir(const float *__restrict__ w, long sc, const float v0[9], const int off[4],
-                                        const float ea[3], float G[3][3], float s[3]) {
+__device__ __forceinline__ void derivs(const Taps &T, const float v0[9], const int off[4], float D[9]) {
+  float t[9];
+  ld9(T, off[0], t);
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    const float d = drp_c<F>(w + (VX + c) * sc, v0[VX + c], off);
-    G[c][0] += ea[0] * d; G[c][1] += ea[1] * d; G[c][2] += ea[2] * d;
+  for (int c = 0; c < 9; c++) D[c] = (F ? kC1 : kC5) * t[c];
+  if (F) {
+#pragma unroll
+    for (int c = 0; c < 9; c++) D[c] += kC2 * v0[c];
   }
-  float d;
-  d = drp_c<F>(w + TXX * sc, v0[TXX], off); s[0] += ea[0] * d;
-  d = drp_c<F>(w + TYY * sc, v0[TYY], off); s[1] += ea[1] * d;
-  d = drp_c<F>(w + TZZ * sc, v0[TZZ], off); s[2] += ea[2] * d;
-  d = drp_c<F>(w + TYZ * sc, v0[TYZ], off); s[1] += ea[2] * d; s[2] += ea[1] * d;
-  d = drp_c<F>(w + TXZ * sc, v0[TXZ], off); s[0] += ea[2] * d; s[2] += ea[0] * d;
-  d = drp_c<F>(w + TXY * sc, v0[TXY], off); s[0] += ea[1] * d; s[1] += ea[0] * d;
+  ld9(T, off[1], t);
+#pragma unroll
+  for (int c = 0; c < 9; c++) D[c] += (F ? kC3 : kC4) * t[c];
+  ld9(T, off[2], t);
+#pragma unroll
+  for (int c = 0; c < 9; c++) D[c] += (F ? kC4 : kC3) * t[c];
+  if (!F) {
+#pragma unroll
+    for (int c = 0; c < 9; c++) D[c] += kC2 * v0[c];
+  }
+  ld9(T, off[3], t);
+#pragma unroll
+  for (int c = 0; c < 9; c++) D[c] = F ? D[c] + kC5 * t[c] : -(D[c] + kC1 * t[c]);
 }
 
+// Accumulate one direction's derivatives straight into the velocity
+// gradient G[c][b] = dV_c/dx_b and the momentum sums
+// s_r = sum_a e_a . d(sigma_row r)/dxi_a.
 template <int F>
-__device__ __forceinline__ void derivs(const float *__restrict__ w, long sc, const float v0[9], const int off[4],
-                                       float D[9]) {
+__device__ __forceinline__ void acc_dir(const Taps &T, const float v0[9], const int off[4], const float ea[3],
+                                        float G[3][3], float s[3]) {
+  float D[9];
+  derivs<F>(T, v0, off, D);
 #pragma unroll
-  for (int c = 0; c < 9; c++) D[c] = drp_c<F>(w + c * sc, v0[c], off);
+  for (int c = 0; c < 3; c++) {
+    const float d = D[VX + c];
+    G[c][0] += ea[0] * d; G[c][1] += ea[1] * d; G[c][2] += ea[2] * d;
+  }
+  s[0] += ea[0] * D[TXX];
+  s[1] += ea[1] * D[TYY];
+  s[2] += ea[2] * D[TZZ];
+  s[1] += ea[2] * D[TYZ]; s[2] += ea[1] * D[TYZ];
+  s[0] += ea[2] * D[TXZ]; s[2] += ea[0] * D[TXZ];
+  s[0] += ea[1] * D[TXY]; s[1] += ea[0] * D[TXY];
 }
 
 // PML face P (normal d) at this point: add its correction to corr and
@@ -182,27 +217,32 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
 // are issued before the first store: the compiler cannot prove that out
 // and end do not alias, and interleaved load / store pairs would cost one
 // memory round trip per component.
+__device__ __forceinline__ void ld9(const float *w, long sc, long p, float v[9], bool ro) {
+  const float4 *A = reinterpret_cast<const float4 *>(w) + p, *B = reinterpret_cast<const float4 *>(w + 4 * sc) + p;
+  const float4 x = ro ? __ldg(A) : *A, y = ro ? __ldg(B) : *B;
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+  v[8] = ro ? __ldg(w + 8 * sc + p) : w[8 * sc + p];
+}
+// level value + k * h at point p of level w
+__device__ __forceinline__ void st9(float *w, long sc, long p, const float v[9], float k, const float h[9]) {
+  reinterpret_cast<float4 *>(w)[p] = make_float4(v[0] + k * h[0], v[1] + k * h[1], v[2] + k * h[2], v[3] + k * h[3]);
+  reinterpret_cast<float4 *>(w + 4 * sc)[p] =
+      make_float4(v[4] + k * h[4], v[5] + k * h[5], v[6] + k * h[6], v[7] + k * h[7]);
+  w[8 * sc + p] = v[8] + k * h[8];
+}
 template <int MODE>
 __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float v0[9], const float h[9]) {
   const long sc = a.g.scmp;
   if (MODE == RK_FIRST) {
-#pragma unroll
-    for (int c = 0; c < 9; c++) {
-      a.out[c * sc + p] = v0[c] + a.ca * h[c];
-      a.end[c * sc + p] = v0[c] + a.cb * h[c];
-    }
+    st9(a.out, sc, p, v0, a.ca, h);
+    st9(a.end, sc, p, v0, a.cb, h);
   } else {
     float pv[9], ev[9];
-#pragma unroll
-    for (int c = 0; c < 9; c++) {
-      if (MODE == RK_MID) pv[c] = __ldg(a.pre + c * sc + p);
-      ev[c] = a.end[c * sc + p];
-    }
-#pragma unroll
-    for (int c = 0; c < 9; c++) {
-      if (MODE == RK_MID) a.out[c * sc + p] = pv[c] + a.ca * h[c];
-      a.end[c * sc + p] = ev[c] + a.cb * h[c];
-    }
+    if (MODE == RK_MID) ld9(a.pre, sc, p, pv, true);
+    ld9(a.end, sc, p, ev, false);
+    if (MODE == RK_MID) st9(a.out, sc, p, pv, a.ca, h);
+    st9(a.end, sc, p, ev, a.cb, h);
   }
 }
 
@@ -279,10 +319,9 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   }
   const long p = g.at(I, J, K);
   const long sc = g.scmp;
-  const float *__restrict__ w = a.cur + p;
+  const Taps w = taps_at(a.cur, sc, p);
   float v0[9];
-#pragma unroll
-  for (int c = 0; c < 9; c++) v0[c] = __ldg(w + c * sc);
+  ld9(w, 0, v0);
   float e[3][3];
 #pragma unroll
   for (int q = 0; q < 9; q++) e[q / 3][q % 3] = __ldg(a.met + (1 + q) * sc + p);
@@ -297,9 +336,9 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   if (KIND == INTERIOR) {
     float G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
     float s[3] = { 0.f, 0.f, 0.f };
-    acc_dir<ID>(w, sc, v0, ox, e[0], G, s);
-    acc_dir<JD>(w, sc, v0, oy, e[1], G, s);
-    acc_dir<KD>(w, sc, v0, oz, e[2], G, s);
+    acc_dir<ID>(w, v0, ox, e[0], G, s);
+    acc_dir<JD>(w, v0, oy, e[1], G, s);
+    acc_dir<KD>(w, v0, oz, e[2], G, s);
     h[VX] = slw * s[0]; h[VY] = slw * s[1]; h[VZ] = slw * s[2];
     h[TXX] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]);
     h[TYY] = l2m * G[1][1] + lam * (G[0][0] + G[2][2]);
@@ -319,11 +358,11 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     constexpr int FF = FD == 0 ? ID : (FD == 1 ? JD : KD);
     float G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
     float s[3] = { 0.f, 0.f, 0.f };
-    if (FD != 0) acc_dir<ID>(w, sc, v0, ox, e[0], G, s);
-    if (FD != 1) acc_dir<JD>(w, sc, v0, oy, e[1], G, s);
-    if (FD != 2) acc_dir<KD>(w, sc, v0, oz, e[2], G, s);
+    if (FD != 0) acc_dir<ID>(w, v0, ox, e[0], G, s);
+    if (FD != 1) acc_dir<JD>(w, v0, oy, e[1], G, s);
+    if (FD != 2) acc_dir<KD>(w, v0, oz, e[2], G, s);
     float D[9], r[9], corr[9];
-    derivs<FF>(w, sc, v0, FD == 0 ? ox : (FD == 1 ? oy : oz), D);
+    derivs<FF>(w, v0, FD == 0 ? ox : (FD == 1 ? oy : oz), D);
     rhs_dir(D, e[FD], lam, mu, l2m, slw, r);
     h[VX] = slw * s[0] + r[VX]; h[VY] = slw * s[1] + r[VY]; h[VZ] = slw * s[2] + r[VZ];
     h[TXX] = l2m * G[0][0] + lam * (G[1][1] + G[2][2]) + r[TXX];
@@ -351,7 +390,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
 #pragma unroll
   for (int c = 0; c < 9; c++) corr[c] = 0.f;
   // x
-  derivs<ID>(w, sc, v0, ox, D);
+  derivs<ID>(w, v0, ox, D);
   dvx[0] = D[VX]; dvx[1] = D[VY]; dvx[2] = D[VZ];
   rhs_dir(D, e[0], lam, mu, l2m, slw, r);
 #pragma unroll
@@ -359,7 +398,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   if (a.pml[0].on) pml_face<MODE>(a, a.pml[0], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
   if (a.pml[1].on) pml_face<MODE>(a, a.pml[1], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
   // y
-  derivs<JD>(w, sc, v0, oy, D);
+  derivs<JD>(w, v0, oy, D);
   dvy[0] = D[VX]; dvy[1] = D[VY]; dvy[2] = D[VZ];
   rhs_dir(D, e[1], lam, mu, l2m, slw, r);
 #pragma unroll
@@ -367,7 +406,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   if (a.pml[2].on) pml_face<MODE>(a, a.pml[2], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
   if (a.pml[3].on) pml_face<MODE>(a, a.pml[3], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
   // z
-  derivs<KD>(w, sc, v0, oz, D);
+  derivs<KD>(w, v0, oz, D);
   rhs_dir(D, e[2], lam, mu, l2m, slw, r);
   if (a.pml[4].on) pml_face<MODE>(a, a.pml[4], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
   if (a.pml[5].on) pml_face<MODE>(a, a.pml[5], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
@@ -384,9 +423,12 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
       mv3(X, dvx, o1); mv3(Y, dvy, o2);
       dz[0] = o1[0] + o2[0]; dz[1] = o1[1] + o2[1]; dz[2] = o1[2] + o2[2];
     } else if (K == nk2 - 1) {
-      dz[0] = mac22(w + VX * sc, sz, KD); dz[1] = mac22(w + VY * sc, sz, KD); dz[2] = mac22(w + VZ * sc, sz, KD);
+      // velocities are components 0-2 of the first group: stride 4 floats
+      const float *v = a.cur + 4 * p;
+      dz[0] = mac22(v + VX, 4 * sz, KD); dz[1] = mac22(v + VY, 4 * sz, KD); dz[2] = mac22(v + VZ, 4 * sz, KD);
     } else {
-      dz[0] = mac24(w + VX * sc, sz, KD); dz[1] = mac24(w + VY * sc, sz, KD); dz[2] = mac24(w + VZ * sc, sz, KD);
+      const float *v = a.cur + 4 * p;
+      dz[0] = mac24(v + VX, 4 * sz, KD); dz[1] = mac24(v + VY, 4 * sz, KD); dz[2] = mac24(v + VZ, 4 * sz, KD);
     }
     float Dz[9], rz[9];
 #pragma unroll
@@ -410,15 +452,15 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     for (int rr = 0; rr < 3; rr++) {
       float dx = 0.f, dy = 0.f, dzz = 0.f;
 #pragma unroll
-      for (int n = 0; n < 5; n++) dx += wdrp<ID>(n) * ctrac(cur, a.met, sc, p + (ID ? n - 1 : n - 3), MXIX, rr);
+      for (int n = 0; n < 5; n++) dx += wdrp<ID>(n) * ctrac(g, cur, a.met, p + (ID ? n - 1 : n - 3), MXIX, rr);
 #pragma unroll
-      for (int n = 0; n < 5; n++) dy += wdrp<JD>(n) * ctrac(cur, a.met, sc, p + (JD ? n - 1 : n - 3) * sy, METX, rr);
+      for (int n = 0; n < 5; n++) dy += wdrp<JD>(n) * ctrac(g, cur, a.met, p + (JD ? n - 1 : n - 3) * sy, METX, rr);
 #pragma unroll
       for (int n = 0; n < 5; n++) {
         const int kk = K + (KD ? n - 1 : n - 3);
         float v = 0.f;
-        if (kk < nk2) v = ctrac(cur, a.met, sc, g.at(I, J, kk), MZTX, rr);
-        else if (kk > nk2) v = -ctrac(cur, a.met, sc, g.at(I, J, 2 * nk2 - kk), MZTX, rr);
+        if (kk < nk2) v = ctrac(g, cur, a.met, g.at(I, J, kk), MZTX, rr);
+        else if (kk > nk2) v = -ctrac(g, cur, a.met, g.at(I, J, 2 * nk2 - kk), MZTX, rr);
         dzz += wdrp<KD>(n) * v;
       }
       h[VX + rr] = (dx + dy + dzz) * sj;
