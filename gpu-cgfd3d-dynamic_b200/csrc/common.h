@@ -86,8 +86,9 @@ struct PmlFaceDev {
   int fni, fnj, fnk;     // face region extents
   long siz;              // fni*fnj*fnk
   const float *A, *B, *D;   // per layer along the normal
-  // auxiliary-field levels used by one stage (9*siz floats each): stage
-  // input, time-n level, next-stage output, end accumulator
+  // auxiliary-field levels used by one stage (9*siz floats each, grouped
+  // like a wavefield level with siz points per component): stage input,
+  // time-n level, next-stage output, end accumulator
   const float *acur, *apre;
   float *aout, *aend;
 };

@@ -152,8 +152,25 @@ __device__ __forceinline__ void acc_dir(const Taps &T, const float v0[9], const 
   s[0] += ea[1] * D[TXY]; s[1] += ea[0] * D[TXY];
 }
 
+// the nine components of point p of a level in the grouped layout with
+// sc points per component (read-only data through the non-coherent path)
+__device__ __forceinline__ void ld9(const float *w, long sc, long p, float v[9], bool ro) {
+  const float4 *A = reinterpret_cast<const float4 *>(w) + p, *B = reinterpret_cast<const float4 *>(w + 4 * sc) + p;
+  const float4 x = ro ? __ldg(A) : *A, y = ro ? __ldg(B) : *B;
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+  v[8] = ro ? __ldg(w + 8 * sc + p) : w[8 * sc + p];
+}
+// level value + k * h at point p of level w
+__device__ __forceinline__ void st9(float *w, long sc, long p, const float v[9], float k, const float h[9]) {
+  reinterpret_cast<float4 *>(w)[p] = make_float4(v[0] + k * h[0], v[1] + k * h[1], v[2] + k * h[2], v[3] + k * h[3]);
+  reinterpret_cast<float4 *>(w + 4 * sc)[p] =
+      make_float4(v[4] + k * h[4], v[5] + k * h[5], v[6] + k * h[6], v[7] + k * h[7]);
+  w[8 * sc + p] = v[8] + k * h[8];
+}
 // PML face P (normal d) at this point: add its correction to corr and
-// advance its auxiliary fields
+// advance its auxiliary fields (stored like a wavefield level, grouped,
+// with P.siz points per component)
 template <int MODE>
 __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, int d, int I, int J, int K,
                                          const float r[9], const float D[9], const float e2[3], float lam,
@@ -163,12 +180,12 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
   const int layer = d == 0 ? li : (d == 1 ? lj : lk);
   const float cA = __ldg(P.A + layer), cB = __ldg(P.B + layer), cD = __ldg(P.D + layer);
   const long pa = li + (long)lj * P.fni + (long)lk * P.fni * P.fnj;
-  float ar[9];
+  float ac[9], ar[9];
+  ld9(P.acur, P.siz, pa, ac, true);
 #pragma unroll
   for (int c = 0; c < 9; c++) {
-    const float av = __ldg(P.acur + c * P.siz + pa);
-    corr[c] += (cB - 1.0f) * r[c] - cB * av;
-    ar[c] = cD * r[c] - cA * av;
+    corr[c] += (cB - 1.0f) * r[c] - cB * ac[c];
+    ar[c] = cD * r[c] - cA * ac[c];
   }
   if (surf) {
     // free-surface coupling of the x / y faces: the d-derivative of the
@@ -188,28 +205,15 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
     for (int c = TXX; c <= TXY; c++) { corr[c] += (cB - 1.0f) * q[c]; ar[c] += cD * q[c]; }
   }
   // auxiliary RK update; level reads first (see rk_update)
-  float av[9], ev[9];
-#pragma unroll
-  for (int c = 0; c < 9; c++) {
-    const long o = c * P.siz + pa;
-    if (MODE == RK_FIRST) av[c] = __ldg(P.acur + o);
-    else {
-      if (MODE == RK_MID) av[c] = __ldg(P.apre + o);
-      ev[c] = P.aend[o];
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < 9; c++) {
-    const long o = c * P.siz + pa;
-    if (MODE == RK_FIRST) {
-      P.aout[o] = av[c] + a.ca * ar[c];
-      P.aend[o] = av[c] + a.cb * ar[c];
-    } else if (MODE == RK_MID) {
-      P.aout[o] = av[c] + a.ca * ar[c];
-      P.aend[o] = ev[c] + a.cb * ar[c];
-    } else {
-      P.aend[o] = ev[c] + a.cb * ar[c];
-    }
+  if (MODE == RK_FIRST) {
+    st9(P.aout, P.siz, pa, ac, a.ca, ar);
+    st9(P.aend, P.siz, pa, ac, a.cb, ar);
+  } else {
+    float pv[9], ev[9];
+    if (MODE == RK_MID) ld9(P.apre, P.siz, pa, pv, true);
+    ld9(P.aend, P.siz, pa, ev, false);
+    if (MODE == RK_MID) st9(P.aout, P.siz, pa, pv, a.ca, ar);
+    st9(P.aend, P.siz, pa, ev, a.cb, ar);
   }
 }
 
@@ -217,20 +221,6 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
 // are issued before the first store: the compiler cannot prove that out
 // and end do not alias, and interleaved load / store pairs would cost one
 // memory round trip per component.
-__device__ __forceinline__ void ld9(const float *w, long sc, long p, float v[9], bool ro) {
-  const float4 *A = reinterpret_cast<const float4 *>(w) + p, *B = reinterpret_cast<const float4 *>(w + 4 * sc) + p;
-  const float4 x = ro ? __ldg(A) : *A, y = ro ? __ldg(B) : *B;
-  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-  v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
-  v[8] = ro ? __ldg(w + 8 * sc + p) : w[8 * sc + p];
-}
-// level value + k * h at point p of level w
-__device__ __forceinline__ void st9(float *w, long sc, long p, const float v[9], float k, const float h[9]) {
-  reinterpret_cast<float4 *>(w)[p] = make_float4(v[0] + k * h[0], v[1] + k * h[1], v[2] + k * h[2], v[3] + k * h[3]);
-  reinterpret_cast<float4 *>(w + 4 * sc)[p] =
-      make_float4(v[4] + k * h[4], v[5] + k * h[5], v[6] + k * h[6], v[7] + k * h[7]);
-  w[8 * sc + p] = v[8] + k * h[8];
-}
 template <int MODE>
 __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float v0[9], const float h[9]) {
   const long sc = a.g.scmp;
@@ -463,7 +453,11 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
         else if (kk > nk2) v = -ctrac(g, cur, a.met, g.at(I, J, 2 * nk2 - kk), MZTX, rr);
         dzz += wdrp<KD>(n) * v;
       }
-      h[VX + rr] = (dx + dy + dzz) * sj;
+      // select instead of h[VX + rr]: a runtime index would move h to the stack
+      const float hv = (dx + dy + dzz) * sj;
+      h[VX] = rr == 0 ? hv : h[VX];
+      h[VY] = rr == 1 ? hv : h[VY];
+      h[VZ] = rr == 2 ? hv : h[VZ];
     }
   }
 #pragma unroll
