@@ -72,7 +72,7 @@ struct cgfd_solver {
   int imethod = 2, isfree = 0;
   float dt = 0.f, dtmax = 0.f;
   float *w[4] = {};                     // storage slots of the 4 levels
-  float *met = nullptr, *med = nullptr, *free_mat = nullptr;
+  float *coef = nullptr, *free_mat = nullptr;   // packed metric and medium (13 scmp floats)
   PmlState pml[6];
   std::vector<FaultState> faults;
   StationDev st{};
@@ -182,7 +182,7 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       a = FaultArgs{};
       a.g = s->g; a.F = F.d;
       a.wcur = s->w[scur]; a.wpre = s->w[spre]; a.wout = sout >= 0 ? s->w[sout] : nullptr; a.wend = s->w[send];
-      a.met = s->met; a.med = s->med; a.free_mat = s->free_mat;
+      a.coef = s->coef; a.free_mat = s->free_mat;
       a.fc = F.lev[scur]; a.fp = F.lev[spre]; a.fo = sout >= 0 ? F.lev[sout] : nullptr; a.fe = F.lev[send];
       a.idir = idir; a.jdir = jdir; a.kdir = kdir; a.mode = mode;
       a.ca = ca; a.cb = cb; a.rkb = kRkB[stage]; a.dt = s->dt;
@@ -205,7 +205,7 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
     VolArgs v{};
     v.g = s->g; v.cur = s->w[scur]; v.pre = s->w[spre]; v.out = sout >= 0 ? s->w[sout] : nullptr; v.end = s->w[send];
-    v.met = s->met; v.med = s->med; v.free_mat = s->free_mat;
+    v.coef = s->coef; v.free_mat = s->free_mat;
     v.ca = ca; v.cb = cb; v.isfree = s->isfree;
     v.nfault = (int)s->faults.size();
     for (size_t f = 0; f < s->faults.size(); f++) { v.fi0[f] = s->faults[f].d.i0; v.fflag[f] = s->faults[f].flag; }
@@ -325,6 +325,29 @@ int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes) {
   return CGFD_OK;
 }
 
+// the host metric [10][scmp] and medium [3][scmp] as the device block of
+// coef_row / coef_jac: the Jacobian plane, then per direction d the groups
+// (e_d.x, e_d.y, e_d.z, medium d), packed and copied in chunks
+static cudaError_t upload_coef(cgfd_solver *s, const HostSetup &H) {
+  const size_t sc = s->g.scmp;
+  cudaError_t e = cudaMemcpyAsync(s->coef, H.metric.data() + (size_t)MJAC * sc, sc * 4, cudaMemcpyHostToDevice, s->stream);
+  const size_t chunk = (size_t)1 << 22;
+  std::vector<float> buf(4 * std::min(chunk, sc));
+  for (int d = 0; d < 3 && e == cudaSuccess; d++) {
+    const float *ex = H.metric.data() + (size_t)(MXIX + 3 * d) * sc, *m = H.media.data() + (size_t)d * sc;
+    for (size_t q0 = 0; q0 < sc && e == cudaSuccess; q0 += chunk) {
+      const size_t n = std::min(chunk, sc - q0);
+      for (size_t q = 0; q < n; q++) {
+        buf[4 * q] = ex[q0 + q]; buf[4 * q + 1] = ex[sc + q0 + q]; buf[4 * q + 2] = ex[2 * sc + q0 + q];
+        buf[4 * q + 3] = m[q0 + q];
+      }
+      e = cudaMemcpyAsync(s->coef + sc + 4 * (d * sc + q0), buf.data(), n * 16, cudaMemcpyHostToDevice, s->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    }
+  }
+  return e;
+}
+
 int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
   if (!cfg || !out) return fail(CGFD_ERR_ARG, "null argument");
   *out = nullptr;
@@ -360,11 +383,9 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   const size_t lev = (size_t)NCMP * g.scmp, ns = (size_t)g.ny * g.nz;
 #define CK(x, what) do { cudaError_t _e = (x); if (_e != cudaSuccess) { destroy(s); return cuda_fail(_e, what); } } while (0)
   for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
-  CK(dalloc(s, &s->met, H.metric.size()), "metric");
-  CK(dalloc(s, &s->med, H.media.size()), "medium");
+  CK(dalloc(s, &s->coef, 13 * (size_t)g.scmp), "metric");
   CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
-  CK(cudaMemcpyAsync(s->met, H.metric.data(), H.metric.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy metric");
-  CK(cudaMemcpyAsync(s->med, H.media.data(), H.media.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy medium");
+  CK(upload_coef(s, H), "copy metric");
   CK(cudaMemcpyAsync(s->free_mat, H.free_mat.data(), H.free_mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy free");
   for (int d = 0; d < 3; d++) for (int sd = 0; sd < 2; sd++) {
     const PmlHost &P = H.pml[d][sd];

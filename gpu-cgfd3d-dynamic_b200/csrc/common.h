@@ -33,8 +33,19 @@ constexpr int MAXF = 8;          // faults
 enum Cmp { VX = 0, VY, VZ, TXX, TYY, TZZ, TYZ, TXZ, TXY };
 // fault wavefield components [side][comp] (src/forward/fault_wav_t.cu:96-150)
 enum FCmp { FVX = 0, FVY, FVZ, FT2X, FT2Y, FT2Z, FT3X, FT3Y, FT3Z };
-// metric component order in the metric block
+// metric component order in the host metric block
 enum Met { MJAC = 0, MXIX, MXIY, MXIZ, METX, METY, METZ, MZTX, MZTY, MZTZ };
+// On the device the metric and the medium are one block of 13 scmp floats:
+// the Jacobian plane, then three arrays of 16-byte groups, one per
+// contravariant direction d, each holding that direction's metric row and
+// one medium value: (xi_x xi_y xi_z lambda), (eta_x eta_y eta_z mu),
+// (zeta_x zeta_y zeta_z 1/rho).
+#ifdef __CUDACC__
+__device__ __forceinline__ float4 coef_row(const float *cf, long scmp, int d, long q) {
+  return __ldg(reinterpret_cast<const float4 *>(cf + scmp) + d * scmp + q);
+}
+__device__ __forceinline__ float coef_jac(const float *cf, long q) { return __ldg(cf + q); }
+#endif
 
 // per-node 3x3 fault matrices, [NFM][nodes][9]
 enum FaultMat {

@@ -47,12 +47,13 @@ namespace {
 
 __device__ __forceinline__ long fidx(int c, int m, long ns, long nd) { return ((long)c * 2 + m) * ns + nd; }
 
-// J * (e_ax . sigma) at point q, 3 components
-__device__ __forceinline__ void trac3(const Grid &g, const float *__restrict__ w, const float *__restrict__ met,
-                                      long q, int ax, float t[3]) {
+// J * (e_d . sigma) at point q, 3 components (d: 0 xi, 1 eta, 2 zeta)
+__device__ __forceinline__ void trac3(const Grid &g, const float *__restrict__ w, const float *__restrict__ cf,
+                                      long q, int d, float t[3]) {
   const long sc = g.scmp;
-  const float J = __ldg(met + MJAC * sc + q);
-  const float ex = __ldg(met + ax * sc + q), ey = __ldg(met + (ax + 1) * sc + q), ez = __ldg(met + (ax + 2) * sc + q);
+  const float J = coef_jac(cf, q);
+  const float4 e = coef_row(cf, sc, d, q);
+  const float ex = e.x, ey = e.y, ez = e.z;
   // Txx ends the first 16-byte group, Tyy Tzz Tyz Txz are the second
   const float sxx = __ldg(w + g.w(TXX, q));
   const float4 s4 = __ldg(reinterpret_cast<const float4 *>(w + 4 * sc) + q);
@@ -94,15 +95,16 @@ __device__ __forceinline__ int trac_slot(int d) { return d < 0 ? d + 6 : d + 5; 
 // split-node volume point from the fault fields (fault2wave_gpu,
 // transform.cu:293-376): velocity = mean of the two sides, stress from the
 // traction vectors [T1 | mean T2 | mean T3] through the inverse metric.
-__device__ void split_to_volume(const Grid &g, const float *__restrict__ met, long sc, long ns, long nd,
+__device__ void split_to_volume(const Grid &g, const float *__restrict__ cf, long sc, long ns, long nd,
                                 int i0, int J, int K, const float *f, const float T1[3], float *wt) {
   const long p0 = g.at(i0, J, K);
   float mt[3][3];   // columns e_xi, e_eta, e_zeta
 #pragma unroll
-  for (int r = 0; r < 3; r++)
-#pragma unroll
-    for (int c = 0; c < 3; c++) mt[r][c] = __ldg(met + (1 + 3 * c + r) * sc + p0);
-  const float rj = 1.0f / __ldg(met + MJAC * sc + p0);
+  for (int c = 0; c < 3; c++) {
+    const float4 e = coef_row(cf, sc, c, p0);
+    mt[0][c] = e.x; mt[1][c] = e.y; mt[2][c] = e.z;
+  }
+  const float rj = 1.0f / coef_jac(cf, p0);
   float tr[3][3];
 #pragma unroll
   for (int r = 0; r < 3; r++) {
@@ -147,8 +149,8 @@ __global__ void k_fault_weld(const FaultArgs a) {
   const long p = g.at(a.F.i0, J, K);
   const float *w = a.wcur;
   float t2[3], t3[3];
-  trac3(g, w, a.met, p, METX, t2);
-  trac3(g, w, a.met, p, MZTX, t3);
+  trac3(g, w, a.coef, p, 1, t2);
+  trac3(g, w, a.coef, p, 2, t3);
   float *f = const_cast<float *>(a.fc);
 #pragma unroll
   for (int m = 0; m < 2; m++) {
@@ -180,12 +182,12 @@ __global__ void __launch_bounds__(192) k_fault_trac(const FaultArgs a) {
   const long q = g.at(a.F.i0 + d, a.tj0 + jj, a.tk0 + kk);
   float *tp = a.trac + node * 12 + slot;
   float v[3];
-  trac3(g, a.wcur, a.met, q, MXIX, v);
+  trac3(g, a.wcur, a.coef, q, 0, v);
   tp[0] = v[0]; tp[pl] = v[1]; tp[2 * pl] = v[2];
   if (d >= -3 && d <= 3) {
-    trac3(g, a.wcur, a.met, q, METX, v);
+    trac3(g, a.wcur, a.coef, q, 1, v);
     tp[3 * pl] = v[0]; tp[4 * pl] = v[1]; tp[5 * pl] = v[2];
-    trac3(g, a.wcur, a.met, q, MZTX, v);
+    trac3(g, a.wcur, a.coef, q, 2, v);
     tp[6 * pl] = v[0]; tp[7 * pl] = v[1]; tp[8 * pl] = v[2];
   }
 }
@@ -206,7 +208,7 @@ __global__ void __launch_bounds__(128) k_fault_trial(const FaultArgs a) {
   const uint8_t fl = F.flag[nd];
   if (!(fl & FL_SPLIT)) return;
   const int i0 = F.i0;
-  const float *met = a.met;
+  const float *cf = a.coef;
   const long ny = g.ny;
   const int km = g.nk - (k + 1);
   const bool surf = a.isfree && km <= 3;
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(128) k_fault_trial(const FaultArgs a) {
 
   // trial traction from the velocity jump of time level n and friction
   const long p0 = g.at(i0, J, K);
-  const float jac0 = __ldg(met + MJAC * sc + p0);
+  const float jac0 = coef_jac(cf, p0);
   const float rho0 = F.scal[FS_RHO0 * ns + nd], rho1 = F.scal[FS_RHO1 * ns + nd];
   const float M0 = 0.5f * jac0 * rho0, M1 = 0.5f * jac0 * rho1;
   float Tr[3];
@@ -263,7 +265,8 @@ __global__ void __launch_bounds__(128) k_fault_trial(const FaultArgs a) {
     const float dV = a.fp[fidx(FVX + c, 1, ns, nd)] - a.fp[fidx(FVX + c, 0, ns, nd)];
     Tr[c] = 2.0f * (M0 * M1 * dV / a.dt + M0 * R[1][c] - M1 * R[0][c]) / (kA0 * (M0 + M1));
   }
-  float vn[3] = { __ldg(met + MXIX * sc + p0), __ldg(met + MXIY * sc + p0), __ldg(met + MXIZ * sc + p0) };
+  const float4 exi = coef_row(cf, sc, 0, p0);
+  float vn[3] = { exi.x, exi.y, exi.z };
   const float vn0 = sqrtf(vn[0] * vn[0] + vn[1] * vn[1] + vn[2] * vn[2]);
   const float jacvec = jac0 * vn0;
   vn[0] /= vn0; vn[1] /= vn0; vn[2] /= vn0;
@@ -298,7 +301,7 @@ __global__ void __launch_bounds__(128) k_fault_trial(const FaultArgs a) {
   // the stage input level sees the new split-node traction before the volume
   // kernel reads it (drv_rk_curv_col.cu:285, fault2wave on w_cur); no fault
   // kernel reads the volume at i0
-  split_to_volume(g, met, sc, ns, nd, i0, J, K, a.fc, T1s, const_cast<float *>(a.wcur));
+  split_to_volume(g, cf, sc, ns, nd, i0, J, K, a.fc, T1s, const_cast<float *>(a.wcur));
   {
     const float s1[3] = { F.scal[FS_S1X * ns + nd], F.scal[FS_S1Y * ns + nd], F.scal[FS_S1Z * ns + nd] };
     const float s2[3] = { F.scal[FS_S2X * ns + nd], F.scal[FS_S2Y * ns + nd], F.scal[FS_S2Z * ns + nd] };
@@ -395,7 +398,7 @@ __global__ void __launch_bounds__(192) k_fault_vslab(const FaultArgs a) {
 
   // y and z lines of T2 = J e_eta . sigma and T3 = J e_zeta . sigma
   const float *t2 = tr + 3 * pl + trac_slot(s), *t3 = t2 + 3 * pl;
-  const float rr = __ldg(a.med + 2 * sc + q) / __ldg(a.met + MJAC * sc + q);
+  const float rr = coef_row(a.coef, sc, 2, q).w / coef_jac(a.coef, q);
   long o[3];
   float h[3];
 #pragma unroll
@@ -430,7 +433,7 @@ __global__ void __launch_bounds__(192) k_fault_sslab(const FaultArgs a) {
   const FaultDev &F = a.F;
   if (!(F.flag[nd] & FL_SPLIT)) return;
   const int i0 = F.i0;
-  const float *w = a.wcur, *met = a.met;
+  const float *w = a.wcur;
   // velocity components sit 4 floats apart from one point to the next
   const long sy = 4 * g.sy, sz = 4 * g.sz;
   const int km = g.nk - (k + 1);
@@ -476,10 +479,9 @@ __global__ void __launch_bounds__(192) k_fault_sslab(const FaultArgs a) {
 #pragma unroll
     for (int c = 0; c < 3; c++) dz[c] = o1[c] + o2[c];
   }
-  float e[3][3];
-#pragma unroll
-  for (int r = 0; r < 9; r++) e[r / 3][r % 3] = __ldg(met + (1 + r) * sc + q);
-  const float lam = __ldg(a.med + q), mu = __ldg(a.med + sc + q);
+  const float4 r0 = coef_row(a.coef, sc, 0, q), r1 = coef_row(a.coef, sc, 1, q), r2 = coef_row(a.coef, sc, 2, q);
+  const float e[3][3] = { { r0.x, r0.y, r0.z }, { r1.x, r1.y, r1.z }, { r2.x, r2.y, r2.z } };
+  const float lam = r0.w, mu = r1.w;
   const float l2m = lam + 2.0f * mu;
   float G[3][3];
 #pragma unroll
@@ -517,7 +519,7 @@ __global__ void __launch_bounds__(128) k_fault_node(const FaultArgs a) {
   const uint8_t fl = F.flag[nd];
   if (!(fl & FL_SPLIT)) return;
   const int i0 = F.i0;
-  const float *w = a.wcur, *met = a.met;
+  const float *w = a.wcur;
   const long ny = g.ny;
   const int km = g.nk - (k + 1);
   const bool fwd = a.idir == 1;
@@ -636,7 +638,7 @@ __global__ void __launch_bounds__(128) k_fault_node(const FaultArgs a) {
   {
     const bool last = a.mode == RK_LAST;
     const float T1s[3] = { F.scal[FS_T1X * ns + nd], F.scal[FS_T1Y * ns + nd], F.scal[FS_T1Z * ns + nd] };
-    split_to_volume(g, met, sc, ns, nd, i0, J, K, last ? a.fe : a.fo, T1s, last ? a.wend : a.wout);
+    split_to_volume(g, a.coef, sc, ns, nd, i0, J, K, last ? a.fe : a.fo, T1s, last ? a.wend : a.wout);
   }
 
   // end of step: slip rate, slip, traction rate, peak slip rate, rupture time

@@ -74,7 +74,7 @@ struct VolArgs {
   VolBox box[12];
   const float *cur, *pre;
   float *out, *end;            // next-stage level (null at the last stage), E
-  const float *met, *med, *free_mat;
+  const float *coef, *free_mat;   // packed metric and medium (coef_row / coef_jac)
   float ca, cb;
   int isfree;
   int nfault;
@@ -88,7 +88,7 @@ struct FaultArgs {
   FaultDev F;
   const float *wcur, *wpre;
   float *wout, *wend;
-  const float *met, *med, *free_mat;
+  const float *coef, *free_mat;   // packed metric and medium (coef_row / coef_jac)
   // fault wavefield levels [9][2 sides][ny*nz]: stage input, time-n level,
   // next-stage output (null at the last stage), end accumulator
   const float *fc, *fp;

@@ -40,18 +40,16 @@ namespace {
 constexpr int BX = 32, BY = 8;
 
 
-// conservative traction J * (e . sigma_row) at point q for metric row `ax`
-// (MXIX, METX or MZTX) and stress row r (0: xx,xy,xz; 1: xy,yy,yz;
+// conservative traction J * (e . sigma_row) at point q for metric row d
+// (0: xi, 1: eta, 2: zeta) and stress row r (0: xx,xy,xz; 1: xy,yy,yz;
 // 2: xz,yz,zz)
-__device__ __forceinline__ float ctrac(const Grid &g, const float *__restrict__ w, const float *__restrict__ met,
-                                       long q, int ax, int r) {
-  const long sc = g.scmp;
+__device__ __forceinline__ float ctrac(const Grid &g, const float *__restrict__ w, const float *__restrict__ cf,
+                                       long q, int d, int r) {
   const int c0 = r == 0 ? TXX : (r == 1 ? TXY : TXZ);
   const int c1 = r == 0 ? TXY : (r == 1 ? TYY : TYZ);
   const int c2 = r == 0 ? TXZ : (r == 1 ? TYZ : TZZ);
-  return __ldg(met + MJAC * sc + q) * (__ldg(met + ax * sc + q) * __ldg(w + g.w(c0, q)) +
-                                       __ldg(met + (ax + 1) * sc + q) * __ldg(w + g.w(c1, q)) +
-                                       __ldg(met + (ax + 2) * sc + q) * __ldg(w + g.w(c2, q)));
+  const float4 e = coef_row(cf, g.scmp, d, q);
+  return coef_jac(cf, q) * (e.x * __ldg(w + g.w(c0, q)) + e.y * __ldg(w + g.w(c1, q)) + e.z * __ldg(w + g.w(c2, q)));
 }
 
 // the point's three groups within one level
@@ -312,10 +310,9 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   const Taps w = taps_at(a.cur, sc, p);
   float v0[9];
   ld9(w, 0, v0);
-  float e[3][3];
-#pragma unroll
-  for (int q = 0; q < 9; q++) e[q / 3][q % 3] = __ldg(a.met + (1 + q) * sc + p);
-  const float lam = __ldg(a.med + p), mu = __ldg(a.med + sc + p), slw = __ldg(a.med + 2 * sc + p);
+  const float4 r0 = coef_row(a.coef, sc, 0, p), r1 = coef_row(a.coef, sc, 1, p), r2 = coef_row(a.coef, sc, 2, p);
+  const float e[3][3] = { { r0.x, r0.y, r0.z }, { r1.x, r1.y, r1.z }, { r2.x, r2.y, r2.z } };
+  const float lam = r0.w, mu = r1.w, slw = r2.w;
   const float l2m = lam + 2.0f * mu;
   int ox[4], oy[4], oz[4];
   tap_offsets<ID>(1, ox);
@@ -437,20 +434,20 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     // traction image on the momentum equation in the top rows
     const float *cur = a.cur;
     const long sy = g.sy;
-    const float sj = slw / __ldg(a.met + MJAC * sc + p);
+    const float sj = slw / coef_jac(a.coef, p);
 #pragma unroll 1
     for (int rr = 0; rr < 3; rr++) {
       float dx = 0.f, dy = 0.f, dzz = 0.f;
 #pragma unroll
-      for (int n = 0; n < 5; n++) dx += wdrp<ID>(n) * ctrac(g, cur, a.met, p + (ID ? n - 1 : n - 3), MXIX, rr);
+      for (int n = 0; n < 5; n++) dx += wdrp<ID>(n) * ctrac(g, cur, a.coef, p + (ID ? n - 1 : n - 3), 0, rr);
 #pragma unroll
-      for (int n = 0; n < 5; n++) dy += wdrp<JD>(n) * ctrac(g, cur, a.met, p + (JD ? n - 1 : n - 3) * sy, METX, rr);
+      for (int n = 0; n < 5; n++) dy += wdrp<JD>(n) * ctrac(g, cur, a.coef, p + (JD ? n - 1 : n - 3) * sy, 1, rr);
 #pragma unroll
       for (int n = 0; n < 5; n++) {
         const int kk = K + (KD ? n - 1 : n - 3);
         float v = 0.f;
-        if (kk < nk2) v = ctrac(g, cur, a.met, g.at(I, J, kk), MZTX, rr);
-        else if (kk > nk2) v = -ctrac(g, cur, a.met, g.at(I, J, 2 * nk2 - kk), MZTX, rr);
+        if (kk < nk2) v = ctrac(g, cur, a.coef, g.at(I, J, kk), 2, rr);
+        else if (kk > nk2) v = -ctrac(g, cur, a.coef, g.at(I, J, 2 * nk2 - kk), 2, rr);
         dzz += wdrp<KD>(n) * v;
       }
       // select instead of h[VX + rr]: a runtime index would move h to the stack
