@@ -19,7 +19,7 @@ NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 # (source, object, extra flags): the volume kernels build as one unit per
 # kernel kind so that they compile in parallel
 CU = [("volume.cu", f"volume_k{k}.cu.o", [f"-DCGFD_VOLUME_KIND={k}"]) for k in range(5)] + [
-    (f, f + ".o", []) for f in ("fault.cu", "noalloc.cu", "api.cu")]
+    (f, f + ".o", []) for f in ("fault.cu", "boundary.cu", "noalloc.cu", "api.cu")]
 CPP = ["setup.cpp"]
 DRIVER = os.path.join(HERE, "driver")
 DRIVER_SRC = ["cgfd_run.cpp", "ncclassic.cpp", "sac.cpp"]

@@ -28,6 +28,9 @@ GRID_IMPORT = 1
 FAULT_FIELDS = ["Tn", "Ts1", "Ts2", "Vs", "Vs1", "Vs2", "Slip", "Slip1", "Slip2",
                 "Peak_vs", "Init_t0"]
 WAVE_COMPONENTS = ["Vx", "Vy", "Vz", "Txx", "Tyy", "Tzz", "Tyz", "Txz", "Txy"]
+# surface peak fields of cgfd_get_surface_peaks (the PG_V_A_D file's variables)
+PEAK_FIELDS = ["PGV", "PGVh", "PGVx", "PGVy", "PGVz", "PGA", "PGAh", "PGAx", "PGAy", "PGAz",
+               "PGD", "PGDh", "PGDx", "PGDy", "PGDz"]
 
 ERRORS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_NOMEM", -4: "ERR_UNSTABLE",
           -5: "ERR_DT", -6: "ERR_NODEVICE", -7: "ERR_STATE"}
@@ -65,6 +68,8 @@ class CgfdConfig(C.Structure):
         ("fault_station_fault", _ip),
         ("fault_station_jk", _fp),
         ("max_records", C.c_int),
+        ("ablexp_layers", (C.c_int * 2) * 3),
+        ("ablexp_ref_vel", (C.c_float * 2) * 3),
     ]
 
 
@@ -102,6 +107,8 @@ class Problem:
     pml_alpha_max: tuple = ((3.14, 3.14), (3.14, 3.14), (3.14, 3.14))
     pml_beta_max: tuple = ((2.0, 2.0), (2.0, 2.0), (2.0, 2.0))
     pml_ref_vel: tuple = ((6000.0, 6000.0), (6000.0, 6000.0), (6000.0, 6000.0))
+    ablexp_layers: tuple = ((0, 0), (0, 0), (0, 0))
+    ablexp_ref_vel: tuple = ((6000.0, 6000.0), (6000.0, 6000.0), (6000.0, 6000.0))
     grid_mode: int = GRID_FAULT_PLANE
     fault_interval: float = 0.0
     fault_x: np.ndarray = None
@@ -146,6 +153,8 @@ class Problem:
                 c.pml_alpha_max[d][s] = float(self.pml_alpha_max[d][s])
                 c.pml_beta_max[d][s] = float(self.pml_beta_max[d][s])
                 c.pml_ref_vel[d][s] = float(self.pml_ref_vel[d][s])
+                c.ablexp_layers[d][s] = int(self.ablexp_layers[d][s])
+                c.ablexp_ref_vel[d][s] = float(self.ablexp_ref_vel[d][s])
         c.grid_mode = int(self.grid_mode)
         c.fault_interval = float(self.fault_interval)
         keep = []
@@ -205,6 +214,7 @@ def load_library(path: str = LIB_PATH):
     lib.cgfd_get_stations.argtypes = [vp, _fp, _ip]
     lib.cgfd_get_fault_stations.argtypes = [vp, _fp, _ip]
     lib.cgfd_get_wavefield.argtypes = [vp, C.c_int, _fp]
+    lib.cgfd_get_surface_peaks.argtypes = [vp, _fp]
     lib.cgfd_set_wavefield.argtypes = [vp, C.c_int, _fp]
     lib.cgfd_checkpoint_size.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     lib.cgfd_checkpoint.argtypes = [vp, vp, C.c_ulonglong]
@@ -361,6 +371,14 @@ class Solver:
         ns = 0 if self.prob.fault_stations is None else len(self.prob.fault_stations)
         out = np.empty((ns, 9, n.value), np.float32)
         self._check(self.lib.cgfd_get_fault_stations(self.h, _fptr(out), C.byref(n)))
+        return out
+
+    def surface_peaks(self):
+        """Peak ground motion of the free surface, [15, nj, ni] in the order
+        of ``PEAK_FIELDS``."""
+        p = self.prob
+        out = np.empty((15, p.nj, p.ni), np.float32)
+        self._check(self.lib.cgfd_get_surface_peaks(self.h, _fptr(out)))
         return out
 
     def wavefield(self, cmp):

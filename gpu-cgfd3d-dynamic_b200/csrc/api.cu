@@ -33,6 +33,8 @@ int launch_fault_post(const FaultArgs &a, cudaStream_t st);
 cudaError_t noalloc_scratch_address(float **p);
 void launch_record(const StationArgs &a, cudaStream_t st);
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
+int launch_sponge(const SpongeArgs &a, cudaStream_t st);
+int launch_surface_peaks(const PeakArgs &a, cudaStream_t st);
 }  // namespace cgfd
 
 using namespace cgfd;
@@ -73,6 +75,9 @@ struct cgfd_solver {
   float dt = 0.f, dtmax = 0.f;
   float *w[4] = {};                     // storage slots of the 4 levels
   float *coef = nullptr, *free_mat = nullptr;   // packed metric and medium (13 scmp floats)
+  float *abl_E = nullptr;               // sponge masks [nx | ny | nz]
+  SpongeArgs sponge{};                  // sponge blocks (w set per step)
+  float *pg = nullptr, *dis = nullptr;  // surface peaks [15][nj][ni], displacement [3][nj][ni]
   PmlState pml[6];
   std::vector<FaultState> faults;
   StationDev st{};
@@ -246,6 +251,19 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     }
     if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
   }
+  // end of step on the time n+1 level: sponge, then the surface peaks
+  // (drv_rk_curv_col.cu:600-613)
+  if (s->sponge.nblk > 0) {
+    SpongeArgs sp = s->sponge;
+    sp.w = s->w[slot(LE, it)];
+    nl += launch_sponge(sp, s->stream);
+  }
+  if (s->isfree) {
+    PeakArgs pa{};
+    pa.g = s->g; pa.wend = s->w[slot(LE, it)]; pa.wpre = s->w[slot(LP, it)];
+    pa.pg = s->pg; pa.dis = s->dis; pa.dt = s->dt;
+    nl += launch_surface_peaks(pa, s->stream);
+  }
   launch_advance(s->ctl, s->st.max_rec, s->stream);
   nl++;
   s->launches_per_step = nl;
@@ -271,6 +289,7 @@ void cgfd_config_default(cgfd_config *c) {
   c->grid_mode = CGFD_GRID_FAULT_PLANE;
   for (int d = 0; d < 3; d++) for (int s = 0; s < 2; s++) {
     c->pml_alpha_max[d][s] = 3.14f; c->pml_beta_max[d][s] = 2.0f; c->pml_ref_vel[d][s] = 6000.f;
+    c->ablexp_ref_vel[d][s] = 6000.f;
   }
 }
 
@@ -387,6 +406,24 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
   CK(upload_coef(s, H), "copy metric");
   CK(cudaMemcpyAsync(s->free_mat, H.free_mat.data(), H.free_mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy free");
+  if (H.abl_nblk > 0) {
+    CK(dalloc(s, &s->abl_E, (size_t)g.nx + g.ny + g.nz), "sponge");
+    CK(cudaMemcpyAsync(s->abl_E, H.abl_E[0].data(), g.nx * 4, cudaMemcpyHostToDevice, s->stream), "copy sponge");
+    CK(cudaMemcpyAsync(s->abl_E + g.nx, H.abl_E[1].data(), g.ny * 4, cudaMemcpyHostToDevice, s->stream), "copy sponge");
+    CK(cudaMemcpyAsync(s->abl_E + g.nx + g.ny, H.abl_E[2].data(), g.nz * 4, cudaMemcpyHostToDevice, s->stream), "copy sponge");
+    SpongeArgs &sp = s->sponge;
+    sp.g = g; sp.E = s->abl_E; sp.nblk = H.abl_nblk;
+    sp.first[0] = 0;
+    for (int b = 0; b < H.abl_nblk; b++) {
+      const int *B = H.abl_blk[b];
+      for (int q = 0; q < 6; q++) sp.blk[b][q] = B[q];
+      sp.first[b + 1] = sp.first[b] + (long)(B[1] - B[0] + 1) * (B[3] - B[2] + 1) * (B[5] - B[4] + 1);
+    }
+  }
+  if (H.isfree) {
+    CK(dalloc(s, &s->pg, (size_t)CGFD_NPEAK * g.ni * g.nj), "surface peaks");
+    CK(dalloc(s, &s->dis, (size_t)3 * g.ni * g.nj), "surface displacement");
+  }
   for (int d = 0; d < 3; d++) for (int sd = 0; sd < 2; sd++) {
     const PmlHost &P = H.pml[d][sd];
     PmlState &S = s->pml[2 * d + sd];
@@ -881,6 +918,15 @@ static CmpArray cmp_array(const Grid &g, int cmp) {
   return { 8 * sc, sc, 1, 0 };
 }
 
+int cgfd_get_surface_peaks(cgfd_solver *s, float *out) {
+  if (!s || !out) return fail(CGFD_ERR_ARG, "bad argument");
+  if (!s->pg) return fail(CGFD_ERR_ARG, "no free surface: no surface peaks");
+  const size_t n = (size_t)CGFD_NPEAK * s->g.ni * s->g.nj;
+  cudaError_t e = cudaMemcpyAsync(out, s->pg, n * 4, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  return e == cudaSuccess ? CGFD_OK : cuda_fail(e, "read surface peaks");
+}
+
 int cgfd_get_wavefield(cgfd_solver *s, int cmp, float *out) {
   if (!s || !out || cmp < 0 || cmp >= NCMP) return fail(CGFD_ERR_ARG, "bad argument");
   const Grid &g = s->g;
@@ -918,6 +964,7 @@ int cgfd_set_wavefield(cgfd_solver *s, int cmp, const float *in) {
 }
 
 // checkpoint: [Ctl][P level][PML P levels][per fault: P level, scal, out, flag][seis][fseis]
+// [surface peaks, surface displacement (free surface only)]
 static std::vector<std::pair<void *, size_t>> state_parts(cgfd_solver *s) {
   std::vector<std::pair<void *, size_t>> v;
   const Grid &g = s->g;
@@ -934,6 +981,10 @@ static std::vector<std::pair<void *, size_t>> state_parts(cgfd_solver *s) {
   }
   v.push_back({ s->seis, (size_t)s->st.n * 9 * std::max(1, s->st.max_rec) * 4 });
   v.push_back({ s->fseis, (size_t)s->st.nf * 9 * std::max(1, s->st.max_rec) * 4 });
+  if (s->pg) {
+    v.push_back({ s->pg, (size_t)CGFD_NPEAK * g.ni * g.nj * 4 });
+    v.push_back({ s->dis, (size_t)3 * g.ni * g.nj * 4 });
+  }
   return v;
 }
 

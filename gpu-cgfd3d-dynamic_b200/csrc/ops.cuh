@@ -116,4 +116,25 @@ struct StationArgs {
   Ctl *ctl;
 };
 
+// exponential sponge on the end-of-step level: masks E[nx | ny | nz]
+// (ghost-inclusive index), blocks of ghost-inclusive inclusive bounds
+// i1 i2 j1 j2 k1 k2, first[b] = points of the blocks before b
+struct SpongeArgs {
+  Grid g;
+  float *w;
+  const float *E;
+  int nblk;
+  int blk[6][6];
+  long first[7];
+};
+
+// peak ground motion of the free surface: end-of-step and time-n levels,
+// peaks [15][nj][ni] and displacement [3][nj][ni] at interior (i, j)
+struct PeakArgs {
+  Grid g;
+  const float *wend, *wpre;
+  float *pg, *dis;
+  float dt;
+};
+
 }  // namespace cgfd

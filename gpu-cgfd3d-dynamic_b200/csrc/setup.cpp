@@ -68,6 +68,18 @@ void extrapolate(float *v, int nx, int ny, int nz, IDX I) {
   }
 }
 
+// bdry_ablexp_cal_mask (src/forward/bdry_t.cu:704-722), in its float
+// arithmetic: alpha spreads a total damping of 0.6 over the steps a wave
+// at `vel` takes to cross the layer
+float ablexp_mask(int i, float vel, float dt, int num_lay, float dh) {
+  const float len = num_lay * dh;
+  const int num_step = (int)(len / vel / dt);
+  float total = 0.0f;
+  for (int n = 0; n < num_step; n++) total += powf((n * dt * vel) / len, 2.0f);
+  const float alpha = (float)(0.6 / total);
+  return expf(-alpha * powf((float)i / num_lay, 2.0f));
+}
+
 }  // namespace
 
 int build_setup(const cgfd_config *c, HostSetup &S, std::string &msg) {
@@ -89,6 +101,19 @@ int build_setup(const cgfd_config *c, HostSetup &S, std::string &msg) {
     int n = d == 0 ? c->ni : (d == 1 ? c->nj : c->nk);
     if (L < 0 || L > n / 2 - 1) { msg = "pml_layers out of range"; return CGFD_ERR_ARG; }
     if (L > 0 && !(c->pml_ref_vel[d][s] > 0.f)) { msg = "pml_ref_vel must be positive"; return CGFD_ERR_ARG; }
+  }
+  {
+    bool any_abl = false, any_pml = false;
+    for (int d = 0; d < 3; d++) for (int s = 0; s < 2; s++) {
+      const int L = c->ablexp_layers[d][s];
+      const int n = d == 0 ? c->ni : (d == 1 ? c->nj : c->nk);
+      if (L < 0 || L > n / 2 - 1) { msg = "ablexp_layers out of range"; return CGFD_ERR_ARG; }
+      if (L > 0 && !(c->ablexp_ref_vel[d][s] > 0.f)) { msg = "ablexp_ref_vel must be positive"; return CGFD_ERR_ARG; }
+      any_abl |= L > 0;
+      any_pml |= c->pml_layers[d][s] > 0;
+    }
+    if (any_abl && any_pml) { msg = "ablexp and cfspml faces cannot be combined"; return CGFD_ERR_ARG; }
+    if (c->free_surface && c->ablexp_layers[2][1] > 0) { msg = "ablexp on the free top face"; return CGFD_ERR_ARG; }
   }
 
   Grid &g = S.g;
@@ -250,6 +275,57 @@ int build_setup(const cgfd_config *c, HostSetup &S, std::string &msg) {
       P.D[idx] = (float)(dd / bb);                  // d / beta
       P.A[idx] = (float)(aa + dd / bb);             // alpha + d / beta
       P.B[idx] = (float)(1.0 / bb);                 // 1 / beta
+    }
+  }
+
+  // ---- exponential sponge (bdry_ablexp_set, bdry_t.cu:453-700): six
+  //      disjoint blocks (x slabs over all y and z, y slabs between them, z
+  //      slabs inside both), each with the mask of its own direction; a
+  //      point is scaled by the smallest of its three masks ------------------
+  S.abl_nblk = 0;
+  for (int d = 0; d < 3; d++) S.abl_E[d].assign(d == 0 ? nx : (d == 1 ? ny : nz), 1.f);
+  {
+    const int (&L)[3][2] = c->ablexp_layers;
+    const int bx0 = ni1 + L[0][0], nbx = g.ni - L[0][0] - L[0][1];
+    const int by0 = nj1 + L[1][0], nby = g.nj - L[1][0] - L[1][1];
+    // [dim][side]: first index and count along each axis
+    const int blk[6][6] = {
+      { ni1, L[0][0], nj1, g.nj, nk1, g.nk }, { ni2 - L[0][1] + 1, L[0][1], nj1, g.nj, nk1, g.nk },
+      { bx0, nbx, nj1, L[1][0], nk1, g.nk }, { bx0, nbx, nj2 - L[1][1] + 1, L[1][1], nk1, g.nk },
+      { bx0, nbx, by0, nby, nk1, L[2][0] }, { bx0, nbx, by0, nby, nk2 - L[2][1] + 1, L[2][1] } };
+    for (int n = 0; n < 6; n++) {
+      const int d = n / 2, side = n % 2;
+      const int *b = blk[n];
+      if (c->ablexp_layers[d][side] <= 0 || b[1] <= 0 || b[3] <= 0 || b[5] <= 0) continue;
+      const int lo[3] = { b[0], b[2], b[4] }, hi[3] = { b[0] + b[1] - 1, b[2] + b[3] - 1, b[4] + b[5] - 1 };
+      // mean spacing along d (bdry_cal_abl_len_dh, bdry_t.cu:329-444): the
+      // reference's loop order, summed in double
+      const int a1 = d == 0 ? 2 : (d == 1 ? 2 : 1), a2 = d == 0 ? 1 : 0;   // outer, middle axes
+      double sum = 0.0;
+      long num = 0;
+      int q[3];
+      for (q[a1] = lo[a1]; q[a1] <= hi[a1]; q[a1]++)
+        for (q[a2] = lo[a2]; q[a2] <= hi[a2]; q[a2]++) {
+          q[d] = lo[d];
+          size_t p0 = U(q[0], q[1], q[2]);
+          double x0 = X[p0], y0 = Y[p0], z0 = Z[p0];
+          for (q[d] = lo[d] + 1; q[d] <= hi[d]; q[d]++) {
+            const size_t p1 = U(q[0], q[1], q[2]);
+            const double x1 = X[p1], y1 = Y[p1], z1 = Z[p1];
+            sum += std::sqrt((x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0) + (z1 - z0) * (z1 - z0));
+            x0 = x1; y0 = y1; z0 = z1;
+            num += 1;
+          }
+        }
+      const float dh = (float)(sum / num);
+      const int nl = b[2 * d + 1];
+      for (int m = lo[d]; m <= hi[d]; m++) {
+        // the first layer inside the domain has the weakest damping
+        const int layer = side == 0 ? nl - (m - lo[d]) : m - lo[d] + 1;
+        S.abl_E[d][m] = ablexp_mask(layer, c->ablexp_ref_vel[d][side], c->dt, nl, dh);
+      }
+      int *o = S.abl_blk[S.abl_nblk++];
+      o[0] = lo[0]; o[1] = hi[0]; o[2] = lo[1]; o[3] = hi[1]; o[4] = lo[2]; o[5] = hi[2];
     }
   }
 

@@ -38,6 +38,12 @@ struct HostSetup {
   std::vector<float> free_mat;    // [2][ny][nx][9]: matVx2Vz, matVy2Vz at the surface
   std::vector<float> coords;      // [3][nk][nj][ni]: x, y, z of the interior grid points
   PmlHost pml[3][2];
+  // exponential sponge: masks along x, y, z (ghost-inclusive index, 1 outside
+  // the layers) and the blocks they scale (ghost-inclusive, inclusive bounds
+  // i1 i2 j1 j2 k1 k2)
+  int abl_nblk = 0;
+  int abl_blk[6][6];
+  std::vector<float> abl_E[3];
   std::vector<FaultHost> faults;
   // stations
   std::vector<long> sta_idx;      // [n][8]

@@ -14,6 +14,9 @@
 //   <station>.<Vx..Txy>.sac     station seismograms (io_funcs.cu:578-617)
 //   fault_<station>.<Tn..Slip2>.sac  fault stations (io_funcs.cu:2355-2400)
 //   <station>.<Exx..Exy>.sac    strain at the stations (io_funcs.cu:620-700)
+//   PG_V_A_D_px0_py0_pz0.nc     peak surface velocity, acceleration and
+//                               displacement with a free surface
+//                               (io_funcs.cu:1827-1880)
 // The time stepping runs in libcgfd (include/cgfd.h).  Par keys of outputs
 // outside the forward path (receiver_line, slice, snapshot, grid / metric /
 // media export) are reported and ignored.
@@ -163,7 +166,10 @@ int main(int argc, char **argv) {
         cfg.pml_beta_max[d][s] = (float)num(*p, "beta_max", 1.0);
         cfg.pml_ref_vel[d][s] = (float)num(*p, "ref_vel", 0.0);
       }
-      if (b->get("ablexp")) die(std::string(bnames[d][s]) + ": the ablexp sponge is not supported (use cfspml)");
+      if (const Value *p = b->get("ablexp")) {
+        cfg.ablexp_layers[d][s] = (int)num(*p, "number_of_layers", 0);
+        cfg.ablexp_ref_vel[d][s] = (float)num(*p, "ref_vel", 0.0);
+      }
       if (d == 2 && s == 1 && b->get("free")) cfg.free_surface = 1;
     }
 
@@ -426,6 +432,33 @@ int main(int argc, char **argv) {
         if (!cgfd_sac::write(out_dir + "/" + sta[r].name + "." + enames[c] + ".sac", T + (size_t)(3 + c) * nrec, nrec,
                              (float)dt, 0, 0, 0, 0, x, y, z, (float)dt))
           die("cannot write SAC files in " + out_dir);
+    }
+  }
+  if (cfg.free_surface) {
+    // peaks on the ghost-inclusive surface plane [ny][nx], zero in the
+    // ghosts, as PG_slice_output writes them
+    const int nx = ni + 6, ny = nj + 6;
+    std::vector<float> pk((size_t)CGFD_NPEAK * ni * nj), plane((size_t)nx * ny);
+    check(cgfd_get_surface_peaks(s, pk.data()), "surface peaks");
+    const char *pnames[CGFD_NPEAK] = { "PGV", "PGVh", "PGVx", "PGVy", "PGVz", "PGA", "PGAh", "PGAx",
+                                       "PGAy", "PGAz", "PGD", "PGDh", "PGDx", "PGDy", "PGDz" };
+    try {
+      cgfd_nc::Writer w(out_dir + "/PG_V_A_D_px0_py0_pz0.nc");
+      const int dj = w.def_dim("j", ny), di = w.def_dim("i", nx);
+      int vid[CGFD_NPEAK];
+      for (int c = 0; c < CGFD_NPEAK; c++) vid[c] = w.def_var(pnames[c], cgfd_nc::FLOAT, { dj, di });
+      w.put_gatt_int("global_index_of_first_physical_points", { 0, 0 });
+      w.put_gatt_int("count_index_of_physical_points", { ni, nj });
+      w.put_gatt_int("coords_of_mpi_topo", { 0, 0, 0 });
+      w.end_define();
+      for (int c = 0; c < CGFD_NPEAK; c++) {
+        for (int j = 0; j < nj; j++)
+          std::memcpy(plane.data() + (size_t)(j + 3) * nx + 3, pk.data() + ((size_t)c * nj + j) * ni, (size_t)ni * 4);
+        w.put_float(vid[c], plane.data());
+      }
+      w.close();
+    } catch (const std::exception &e) {
+      die(e.what());
     }
   }
   cgfd_destroy(s);

@@ -54,6 +54,9 @@ def write_case(prob: Problem, case_dir: str, nt: int, output_dir: str = None, io
     for key, d, s in names:
         if d == 2 and s == 1 and prob.free_surface:
             par[key] = {"free": "timg"}
+        elif prob.ablexp_layers[d][s] > 0:
+            par[key] = {"ablexp": {"number_of_layers": int(prob.ablexp_layers[d][s]),
+                                   "ref_vel": float(prob.ablexp_ref_vel[d][s])}}
         elif prob.pml_layers[d][s] > 0:
             par[key] = {"cfspml": {"number_of_layers": int(prob.pml_layers[d][s]),
                                    "alpha_max": float(prob.pml_alpha_max[d][s]),
@@ -125,6 +128,12 @@ def read_fault_output(path):
         out = {k: np.array(v[:]) for k, v in f.variables.items()}
         out["_attrs"] = dict(f._attributes)
     return out
+
+
+def read_surface_peaks(path):
+    """dict of the PG_V_A_D file's variables [ny][nx] (ghost-inclusive) and
+    its global attributes under "_attrs"."""
+    return read_fault_output(path)
 
 
 def read_sac(path):

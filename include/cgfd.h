@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define CGFD_ABI_VERSION 1
+#define CGFD_ABI_VERSION 2
 
 #define CGFD_MAX_FAULTS 8
 
@@ -130,6 +130,15 @@ typedef struct cgfd_config {
   const float *fault_station_jk;
   /* capacity of the station/fault-station time series (records) */
   int max_records;
+  /* exponential sponge per face [dim][side] ("boundary_*": {"ablexp":
+   * {"number_of_layers", "ref_vel"}}): every step the end-of-step level is
+   * multiplied by exp(-alpha (n/L)^2) in the outer L layers
+   * (bdry_ablexp_set / bdry_ablexp_apply, src/forward/bdry_t.cu:453-818).
+   * 0 layers = no sponge.  Sponge faces cannot be combined with cfspml
+   * faces (the reference then computes masks for the PML faces from an
+   * unset velocity), nor with the free top. */
+  int   ablexp_layers[3][2];
+  float ablexp_ref_vel[3][2];
 } cgfd_config;
 
 typedef struct cgfd_solver cgfd_solver;
@@ -196,6 +205,14 @@ int cgfd_get_stations(cgfd_solver *s, float *out, int *nrec);
 /* Fault-station time series [num_fault_stations][9][nrec] of
  * Tn,Ts1,Ts2,Vs,Vs1,Vs2,Slip,Slip1,Slip2. */
 int cgfd_get_fault_stations(cgfd_solver *s, float *out, int *nrec);
+
+/* Peak ground motion of the free surface over the steps run so far
+ * (PG_calcu_gpu, src/forward/wav_t.cu:138-216): [CGFD_NPEAK][nj][ni] in the
+ * order PGV, PGVh, PGVx, PGVy, PGVz, PGA, PGAh, PGAx, PGAy, PGAz, PGD, PGDh,
+ * PGDx, PGDy, PGDz (the variables of PG_V_A_D_*.nc, io_funcs.cu:1827-1880).
+ * CGFD_ERR_ARG without a free surface. */
+#define CGFD_NPEAK 15
+int cgfd_get_surface_peaks(cgfd_solver *s, float *out);
 
 /* One wavefield component (CGFD_VX..CGFD_TXY) of the current level at
  * interior points, [nk][nj][ni]. */

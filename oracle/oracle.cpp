@@ -214,6 +214,12 @@ struct oracle_solver {
   int max_rec = 0, nrec = 0;
   std::vector<real> seis, fseis;   // [n][9][max_rec]
   real dtmax = 0;
+  // exponential sponge (bdryexp_t): masks along x, y, z and six blocks
+  std::vector<real> abl_Ex, abl_Ey, abl_Ez;
+  struct AblBlock { int enable, ni1, ni, nj1, nj, nk1, nk; } abl_blk[6];
+  int abl_on = 0;
+  // surface peaks [15][ny][nx] and displacement [3][ny][nx] (PG_d, Dis_accu_d)
+  std::vector<real> pg, dis;
 
   size_t I(int i, int j, int k) const { return (size_t)i + (size_t)j*siz_iy + (size_t)k*siz_iz; }
   real *W(int l) { return w[wl[l]].data(); }
@@ -1446,6 +1452,101 @@ void record(oracle_solver *S) {
   S->nrec++;
 }
 
+/* -------- exponential sponge: bdry_ablexp_set (bdry_t.cu:453-700),
+ *          bdry_cal_abl_len_dh (:329-444), bdry_ablexp_cal_mask (:704-722),
+ *          bdry_ablexp_apply_gpu (:764-818) ------------------------------ */
+real abl_mask(int i, real vel, real dt, int num_lay, real dh) {
+  real len = num_lay * dh;
+  int num_step = (int)(len / vel / dt);
+  real total_damp = 0;
+  for (int n = 0; n < num_step; n++) total_damp += std::pow((n*dt*vel)/len, (real)2.0);
+  real alpha = (real)(0.6 / (double)total_damp);
+  return std::exp(-alpha * std::pow((real)i/num_lay, (real)2.0));
+}
+
+// mean spacing of the block along idim, the reference's loop order
+real abl_dh(oracle_solver *S, int i1, int i2, int j1, int j2, int k1, int k2, int idim) {
+  double L = 0.0; int num = 0;
+  auto seg = [&](size_t a, size_t b) {
+    double x0 = S->x3d[a], y0 = S->y3d[a], z0 = S->z3d[a];
+    double x1 = S->x3d[b], y1 = S->y3d[b], z1 = S->z3d[b];
+    L += std::sqrt((x1-x0)*(x1-x0) + (y1-y0)*(y1-y0) + (z1-z0)*(z1-z0)); num += 1;
+  };
+  if (idim == 0) {
+    for (int k = k1; k <= k2; k++) for (int j = j1; j <= j2; j++) for (int i = i1+1; i <= i2; i++) seg(S->I(i-1,j,k), S->I(i,j,k));
+  } else if (idim == 1) {
+    for (int k = k1; k <= k2; k++) for (int i = i1; i <= i2; i++) for (int j = j1+1; j <= j2; j++) seg(S->I(i,j-1,k), S->I(i,j,k));
+  } else {
+    for (int j = j1; j <= j2; j++) for (int i = i1; i <= i2; i++) for (int k = k1+1; k <= k2; k++) seg(S->I(i,j,k-1), S->I(i,j,k));
+  }
+  return (real)(float)(L / num);
+}
+
+void abl_set(oracle_solver *S, const cgfd_config *c) {
+  S->abl_Ex.assign(S->nx, 1); S->abl_Ey.assign(S->ny, 1); S->abl_Ez.assign(S->nz, 1);
+  const int (&nl)[3][2] = c->ablexp_layers;
+  for (int d = 0; d < 3; d++) for (int s = 0; s < 2; s++) if (nl[d][s] > 0) S->abl_on = 1;
+  const int ni_x = nl[0][0] + nl[0][1], nj_y = nl[1][0] + nl[1][1];
+  auto &D = S->abl_blk;
+  // x1, x2, y1, y2, z1, z2
+  D[0] = { 0, S->ni1, nl[0][0], S->nj1, S->nj, S->nk1, S->nk };
+  D[1] = { 0, S->ni2 - nl[0][1] + 1, nl[0][1], S->nj1, S->nj, S->nk1, S->nk };
+  D[2] = { 0, S->ni1 + nl[0][0], S->ni - ni_x, S->nj1, nl[1][0], S->nk1, S->nk };
+  D[3] = { 0, S->ni1 + nl[0][0], S->ni - ni_x, S->nj2 - nl[1][1] + 1, nl[1][1], S->nk1, S->nk };
+  D[4] = { 0, S->ni1 + nl[0][0], S->ni - ni_x, S->nj1 + nl[1][0], S->nj - nj_y, S->nk1, nl[2][0] };
+  D[5] = { 0, S->ni1 + nl[0][0], S->ni - ni_x, S->nj1 + nl[1][0], S->nj - nj_y, S->nk2 - nl[2][1] + 1, nl[2][1] };
+  for (int n = 0; n < 6; n++) {
+    auto &B = D[n];
+    if (!(B.ni > 0 && B.nj > 0 && B.nk > 0)) continue;
+    B.enable = 1;
+    const int d = n / 2, s = n % 2;
+    real dh = abl_dh(S, B.ni1, B.ni1 + B.ni - 1, B.nj1, B.nj1 + B.nj - 1, B.nk1, B.nk1 + B.nk - 1, d);
+    real vel = c->ablexp_ref_vel[d][s];
+    const int lo = d == 0 ? B.ni1 : (d == 1 ? B.nj1 : B.nk1), cnt = d == 0 ? B.ni : (d == 1 ? B.nj : B.nk);
+    std::vector<real> &E = d == 0 ? S->abl_Ex : (d == 1 ? S->abl_Ey : S->abl_Ez);
+    for (int m = lo; m < lo + cnt; m++)
+      E[m] = abl_mask(s == 0 ? cnt - (m - lo) : m - lo + 1, vel, S->dt, cnt, dh);
+  }
+}
+
+void abl_apply(oracle_solver *S, real *w) {
+  const size_t ic = S->siz_icmp;
+  for (int n = 0; n < 6; n++) {
+    const auto &B = S->abl_blk[n];
+    if (!B.enable) continue;
+    for (int iz = 0; iz < B.nk; iz++) for (int iy = 0; iy < B.nj; iy++) for (int ix = 0; ix < B.ni; ix++) {
+      size_t p = S->I(ix + B.ni1, iy + B.nj1, iz + B.nk1);
+      real mask = (S->abl_Ex[ix+B.ni1] < S->abl_Ey[iy+B.nj1]) ? S->abl_Ex[ix+B.ni1] : S->abl_Ey[iy+B.nj1];
+      if (mask > S->abl_Ez[iz+B.nk1]) mask = S->abl_Ez[iz+B.nk1];
+      for (int c = 0; c < 9; c++) w[p + c*ic] *= mask;
+    }
+  }
+}
+
+/* -------- surface peak motion: PG_calcu_gpu (wav_t.cu:138-216) ---------- */
+void pg_calc(oracle_solver *S, const real *w_end, const real *w_pre) {
+  const size_t ic = S->siz_icmp, n = S->siz_iz;
+  const real dt = S->dt;
+  real *PG = S->pg.data(), *Dx = S->dis.data(), *Dy = Dx + n, *Dz = Dx + 2*n;
+  for (int iy = 0; iy < S->nj; iy++) for (int ix = 0; ix < S->ni; ix++) {
+    const size_t p = S->I(ix + S->ni1, iy + S->nj1, S->nk2), q = (size_t)(ix + S->ni1) + (size_t)(iy + S->nj1)*S->siz_iy;
+    const real vx1 = w_end[VX*ic+p], vy1 = w_end[VY*ic+p], vz1 = w_end[VZ*ic+p];
+    const real vx0 = w_pre[VX*ic+p], vy0 = w_pre[VY*ic+p], vz0 = w_pre[VZ*ic+p];
+    real Ax = std::fabs((vx1-vx0)/dt), Ay = std::fabs((vy1-vy0)/dt), Az = std::fabs((vz1-vz0)/dt);
+    // the reference's 0.5 is a double constant
+    Dx[q] = (real)((double)Dx[q] + 0.5*(double)(vx1+vx0)*(double)dt);
+    Dy[q] = (real)((double)Dy[q] + 0.5*(double)(vy1+vy0)*(double)dt);
+    Dz[q] = (real)((double)Dz[q] + 0.5*(double)(vz1+vz0)*(double)dt);
+    const real val[15] = {
+      std::sqrt(vx1*vx1 + vy1*vy1 + vz1*vz1), std::sqrt(vx1*vx1 + vy1*vy1),
+      std::fabs(vx1), std::fabs(vy1), std::fabs(vz1),
+      std::sqrt(Ax*Ax + Ay*Ay + Az*Az), std::sqrt(Ax*Ax + Ay*Ay), Ax, Ay, Az,
+      std::sqrt(Dx[q]*Dx[q] + Dy[q]*Dy[q] + Dz[q]*Dz[q]), std::sqrt(Dx[q]*Dx[q] + Dy[q]*Dy[q]),
+      std::fabs(Dx[q]), std::fabs(Dy[q]), std::fabs(Dz[q]) };
+    for (int c = 0; c < 15; c++) if (PG[c*n + q] < val[c]) PG[c*n + q] = val[c];
+  }
+}
+
 /* one time step: drv_rk_curv_col.cu:209-636 */
 void step(oracle_solver *S) {
   const int it = S->it;
@@ -1527,6 +1628,9 @@ void step(oracle_solver *S) {
     }
     for (auto &F : S->faults) fault_stage_out(S, F, RK_B[istage], istage);
   }
+  // end of step: sponge, surface peaks, fault outputs (drv_rk_curv_col.cu:596-616)
+  if (S->abl_on) abl_apply(S, S->W(LEND));
+  if (S->isfree) pg_calc(S, S->W(LEND), S->W(LPRE));
   for (auto &F : S->faults) fault_step_out(S, F, F.lev(LEND), it);
   std::swap(S->wl[LPRE], S->wl[LEND]);
   for (auto &F : S->faults) std::swap(F.lvl[LPRE], F.lvl[LEND]);
@@ -1594,7 +1698,9 @@ int oracle_create(const cgfd_config *c, oracle_solver **out) {
   for (int f = 0; f < c->num_faults; f++) fault_coef(S, S->faults[f]);
   for (int f = 0; f < c->num_faults; f++) fault_set(S, S->faults[f], c, f, margin);
   pml_set(S, c);
+  abl_set(S, c);
   if (S->isfree) free_set(S);
+  if (S->isfree) { S->pg.assign(15*S->siz_iz, 0); S->dis.assign(3*S->siz_iz, 0); }
   for (size_t q = 0; q < S->siz_icmp; q++) S->rho[q] = S->rho[q] > 1e-10 ? 1.0/S->rho[q] : 0.0;
   for (int l = 0; l < 4; l++) S->w[l].assign(9*S->siz_icmp, 0);
   S->max_rec = c->max_records > 0 ? c->max_records : 0;
@@ -1677,6 +1783,14 @@ int oracle_get_metric(oracle_solver *S, int cmp, float *out) {
   const real *m = S->M(cmp);
   for (int k = 0; k < S->nk; k++) for (int j = 0; j < S->nj; j++) for (int i = 0; i < S->ni; i++)
     out[(size_t)i + (size_t)S->ni*((size_t)j + (size_t)S->nj*k)] = (float)m[S->I(i+3,j+3,k+3)];
+  return CGFD_OK;
+}
+
+int oracle_get_surface_peaks(oracle_solver *S, float *out) {
+  if (!S || !out) return set_err(CGFD_ERR_ARG, "bad argument");
+  if (!S->isfree) return set_err(CGFD_ERR_ARG, "no free surface");
+  for (int c = 0; c < 15; c++) for (int j = 0; j < S->nj; j++) for (int i = 0; i < S->ni; i++)
+    out[((size_t)c*S->nj + j)*S->ni + i] = (float)S->pg[c*S->siz_iz + (size_t)(i+3) + (size_t)(j+3)*S->siz_iy];
   return CGFD_OK;
 }
 

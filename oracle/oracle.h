@@ -29,6 +29,8 @@ int  oracle_get_wavefield(oracle_solver *s, int cmp, float *out);
 int  oracle_set_wavefield(oracle_solver *s, int cmp, const float *in);
 /* metric (0 jac, 1..9 xi_x..zeta_z) at interior points [nk][nj][ni] */
 int  oracle_get_metric(oracle_solver *s, int cmp, float *out);
+/* surface peaks [15][nj][ni] as cgfd_get_surface_peaks */
+int  oracle_get_surface_peaks(oracle_solver *s, float *out);
 int  oracle_dt_max(oracle_solver *s, float *dtmax);
 int  oracle_set_threads(int nthreads);
 int  oracle_real_bytes(void);

@@ -40,6 +40,7 @@ def load(double=False):
     lib.oracle_set_wavefield.argtypes = [vp, C.c_int, _fp]
     lib.oracle_get_metric.argtypes = [vp, C.c_int, _fp]
     lib.oracle_dt_max.argtypes = [vp, _fp]
+    lib.oracle_get_surface_peaks.argtypes = [vp, _fp]
     lib.oracle_set_threads.argtypes = [C.c_int]
     lib.oracle_destroy.argtypes = [vp]
     lib.oracle_destroy.restype = None
@@ -91,6 +92,14 @@ class OracleSolver:
         ns = 0 if self.prob.fault_stations is None else len(self.prob.fault_stations)
         out = np.empty((ns, 9, n.value), np.float32)
         self.lib.oracle_get_fault_stations(self.h, out.ctypes.data_as(_fp), C.byref(n))
+        return out
+
+    def surface_peaks(self):
+        p = self.prob
+        out = np.empty((15, p.nj, p.ni), np.float32)
+        rc = self.lib.oracle_get_surface_peaks(self.h, out.ctypes.data_as(_fp))
+        if rc != 0:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
         return out
 
     def wavefield(self, cmp):

@@ -30,7 +30,7 @@ def test_header_declares_entry_points():
 def test_library_exports_all(cgfd_lib):
     missing = [n for n in declared_functions() if not hasattr(cgfd_lib, n)]
     assert not missing, missing
-    assert cgfd_lib.cgfd_abi_version() == 1
+    assert cgfd_lib.cgfd_abi_version() == 2
 
 
 def test_config_default(cgfd_lib):

@@ -4,6 +4,7 @@ CPU: its netCDF classic reader and writer against scipy's independent
 implementation of the format, its SAC header layout, the JSON reader.
 GPU: a whole run from par.json and reference-format input files, whose
 output files must hold what the library returns for the same problem."""
+import dataclasses
 import json
 import os
 import subprocess
@@ -96,9 +97,10 @@ def _driver():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("medium,case", [("import", "planar"), ("code", "hills"), ("import", "two_faults")])
+@pytest.mark.parametrize("medium,case", [("import", "planar"), ("code", "hills"), ("import", "two_faults"),
+                                         ("import", "sponge")])
 def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, case):
-    from cgfd import Solver
+    from cgfd import PEAK_FIELDS, Solver
     nt, skip = 30, 3
     if case == "two_faults":
         p = inputs.two_faults(nt=nt)
@@ -107,6 +109,9 @@ def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, case):
                                  margin=6, nt=nt, nhills=2)
         lam, mu, rho = inputs._homog(p.ni, p.nj, p.nk)   # the driver's uniform medium
         p.lam, p.mu, p.rho = lam, mu, rho
+    elif case == "sponge":
+        p = dataclasses.replace(inputs.small_planar(nt=nt, pml=0), ablexp_layers=((6, 6), (6, 6), (6, 0)),
+                                ablexp_ref_vel=((6000.0, 6000.0),) * 3)
     else:
         p = inputs.small_planar(nt=nt)
     par = par_files.write_case(p, str(tmp_path / "case"), nt=nt, io_time_skip=skip, medium=medium)
@@ -148,3 +153,17 @@ def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, case):
         for c, name in enumerate(par_files.FAULT_CMP):
             _, _, _, tr = par_files.read_sac(os.path.join(out, f"fault_f{q}.{name}.sac"))
             assert np.array_equal(tr, fseis[q, c]), (q, name)
+    # peak surface motion: the library's values in the interior of the
+    # ghost-inclusive plane, zeros in the ghosts
+    if not p.free_surface:
+        assert not os.path.exists(os.path.join(out, "PG_V_A_D_px0_py0_pz0.nc"))
+        return
+    pg = par_files.read_surface_peaks(os.path.join(out, "PG_V_A_D_px0_py0_pz0.nc"))
+    mine = s.surface_peaks()
+    for c, name in enumerate(PEAK_FIELDS):
+        v = pg[name]
+        assert v.shape == (p.nj + 6, p.ni + 6)
+        assert np.array_equal(v[3:-3, 3:-3], mine[c]), name
+        assert not v[:3].any() and not v[:, :3].any()
+    assert mine[0].max() > 0
+    assert list(np.ravel(pg["_attrs"]["count_index_of_physical_points"])) == [p.ni, p.nj]

@@ -5,11 +5,13 @@ Tolerances: relative L2 <= 1e-4 for slip rate, slip, rupture time and
 station velocity (the bar of the forward path); <= 2e-5 for whole
 wavefields after a few steps from a random state.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
 import inputs
-from cgfd import Solver, WAVE_COMPONENTS
+from cgfd import PEAK_FIELDS, Solver, WAVE_COMPONENTS
 from oracle import OracleSolver
 
 pytestmark = pytest.mark.gpu
@@ -81,12 +83,13 @@ def test_checkpoint_restore(cgfd_lib):
     g.run(13)
     buf = g.checkpoint()
     g.run(20)
-    ref = g.fault("Slip").copy(), g.wavefield("Vy").copy()
+    ref = g.fault("Slip").copy(), g.wavefield("Vy").copy(), g.surface_peaks()
     g.restore(buf)
     assert g.steps_done == 13
     g.run(20)
     assert np.array_equal(g.fault("Slip"), ref[0])
     assert np.array_equal(g.wavefield("Vy"), ref[1])
+    assert np.array_equal(g.surface_peaks(), ref[2])
 
 
 def test_graph_and_direct_launch_agree(cgfd_lib, monkeypatch):
@@ -111,4 +114,80 @@ def test_unstable_run_reports_error(cgfd_lib):
 def test_dt_above_limit_rejected(cgfd_lib):
     p = inputs.small_planar(nt=10, dt=0.05)
     with pytest.raises(Exception, match="ERR_DT"):
+        Solver(p)
+
+
+def _sponge(p, layers=6, vel=6000.0):
+    """The same problem with an exponential sponge on the five non-surface
+    faces in place of the CFS-PML."""
+    top = 0 if p.free_surface else layers
+    return dataclasses.replace(p, pml_layers=((0, 0), (0, 0), (0, 0)),
+                               ablexp_layers=((layers, layers), (layers, layers), (layers, top)),
+                               ablexp_ref_vel=((vel, vel), (vel, vel), (vel, vel)))
+
+
+@pytest.mark.parametrize("free", [1, 0])
+def test_sponge_random_state_steps(cgfd_lib, oracle_built, free):
+    """Eight steps from a random wavefield with the sponge instead of the
+    PML: the end-of-step masks, and with a free surface the surface peaks."""
+    p = _sponge(inputs.small_planar(nt=10, pml=0, free_surface=free))
+    rng = np.random.default_rng(12)
+    g, o = _pair(p)
+    for c in range(9):
+        scale = 1e-3 if c < 3 else 1e3
+        f = (rng.standard_normal((p.nk, p.nj, p.ni)) * scale).astype(np.float32)
+        g.set_wavefield(c, f)
+        o.set_wavefield(c, f)
+    for step in range(8):
+        g.run(1)
+        o.run(1)
+        for c in range(9):
+            e = rel_l2(g.wavefield(c), o.wavefield(c))
+            assert e < 2e-5, f"step {step} {WAVE_COMPONENTS[c]} rel-L2 {e:.2e}"
+    if free:
+        pg, po = g.surface_peaks(), o.surface_peaks()
+        for c, name in enumerate(PEAK_FIELDS):
+            assert rel_l2(pg[c], po[c]) < 2e-5, name
+
+
+def test_rupture_sponge_and_peaks(cgfd_lib, oracle_built):
+    """A rupture with the sponge boundary: fault outputs, stations and the
+    free-surface peak velocity, acceleration and displacement."""
+    nt = 80
+    p = _sponge(inputs.small_planar(nt=nt, pml=0))
+    g, o = _pair(p)
+    g.run(nt)
+    o.run(nt)
+    assert o.fault("Vs").max() > 0.1, "no rupture in the oracle run"
+    for f in ("Vs", "Slip", "Peak_vs", "Tn", "Ts1"):
+        assert rel_l2(g.fault(f), o.fault(f)) < TOL, f
+    assert rel_l2(g.stations()[:, :3], o.stations()[:, :3]) < TOL
+    pg, po = g.surface_peaks(), o.surface_peaks()
+    assert po[0].max() > 0
+    for c, name in enumerate(PEAK_FIELDS):
+        assert rel_l2(pg[c], po[c]) < TOL, name
+
+
+def test_surface_peaks_with_pml(cgfd_lib, oracle_built):
+    """Peaks of the PML case of the rupture tests (the configuration the
+    benchmarks run)."""
+    nt = 60
+    p = inputs.small_planar(nt=nt)
+    g, o = _pair(p)
+    g.run(nt)
+    o.run(nt)
+    pg, po = g.surface_peaks(), o.surface_peaks()
+    for c, name in enumerate(PEAK_FIELDS):
+        assert rel_l2(pg[c], po[c]) < TOL, name
+
+
+def test_no_surface_peaks_without_free_surface(cgfd_lib):
+    g = Solver(inputs.small_planar(nt=10, free_surface=0))
+    with pytest.raises(Exception, match="ERR_ARG"):
+        g.surface_peaks()
+
+
+def test_sponge_with_pml_rejected(cgfd_lib):
+    p = dataclasses.replace(inputs.small_planar(nt=10), ablexp_layers=((4, 4), (0, 0), (0, 0)))
+    with pytest.raises(Exception, match="ERR_ARG"):
         Solver(p)

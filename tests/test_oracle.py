@@ -153,3 +153,52 @@ def test_locked_fault_matches_welded(oracle_built):
     assert vs < 1e-6
     for c in res[False]:
         assert _rel(res[True][c], res[False][c]) < 0.03, c
+
+
+def _sponge_mask_np(layer, vel, dt, nl, dh):
+    """bdry_ablexp_cal_mask (src/forward/bdry_t.cu:704-722) restated in numpy
+    float32, independently of the oracle's C++."""
+    f = np.float32
+    ln = f(nl) * f(dh)
+    num_step = int(ln / f(vel) / f(dt))
+    total = f(0.0)
+    for n in range(num_step):
+        total = f(total + f((f(n) * f(dt) * f(vel)) / ln) ** 2)
+    alpha = f(0.6 / float(total))
+    return float(np.exp(f(-alpha * f(f(layer) / f(nl)) ** 2)))
+
+
+def test_sponge_masks_one_step(oracle_built):
+    """One step from the same random state with and without the sponge: the
+    ratio of the end levels is the mask, 1 outside the layers, the numpy
+    mask formula inside (uniform 200 m grid), smallest at the outer face."""
+    import dataclasses
+    from oracle import OracleSolver
+    L, vel = 6, 5000.0
+    base = inputs.small_planar(nt=2, pml=0)
+    spg = dataclasses.replace(base, ablexp_layers=((L, L), (L, L), (L, 0)),
+                              ablexp_ref_vel=((vel, vel), (vel, vel), (vel, vel)))
+    rng = np.random.default_rng(5)
+    a, b = OracleSolver(base), OracleSolver(spg)
+    for c in range(9):
+        f = (rng.standard_normal((base.nk, base.nj, base.ni)) + 3.0).astype(np.float32)
+        a.set_wavefield(c, f)
+        b.set_wavefield(c, f)
+    a.run(1)
+    b.run(1)
+    wa, wb = a.wavefield("Txx"), b.wavefield("Txx")
+    ratio = wb / wa
+    ni, nj, nk = base.ni, base.nj, base.nk
+    jm, km = nj // 2, nk // 2
+    mask = [_sponge_mask_np(L - i, vel, base.dt, L, 200.0) for i in range(L)]
+    # x-left layers along one line through the middle of the y-z face
+    np.testing.assert_allclose(ratio[km, jm, :L], mask, rtol=3e-6)
+    np.testing.assert_allclose(ratio[km, jm, ni - L:], mask[::-1], rtol=3e-6)
+    np.testing.assert_allclose(ratio[km, :L, ni // 2], mask, rtol=3e-6)
+    np.testing.assert_allclose(ratio[:L, jm, ni // 2], mask, rtol=3e-6)
+    assert mask[0] < mask[-1] < 1.0
+    # no damping under the free top or inside the layers' inner faces
+    inner = ratio[L:, L:nj - L, L:ni - L]
+    assert np.array_equal(inner, np.ones_like(inner))
+    # a corner point takes the smallest of its masks
+    np.testing.assert_allclose(ratio[0, 0, 0], mask[0], rtol=3e-6)
