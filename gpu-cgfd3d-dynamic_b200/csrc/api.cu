@@ -94,9 +94,11 @@ struct cgfd_solver {
   cudaEvent_t ev_vol[8][4][2] = {};
   cudaEvent_t ev_int[8][4] = {};        // after the interior-box kernel
   cudaEvent_t ev_int0[8][4] = {};       // before it
-  // concurrent branches of a stage (fault slabs and nodes, PML slabs and
-  // shell beside the interior kernel): streams and fork / join events
-  int branches = 0;                     // CGFD_BRANCHES=1: measured +1.3% on the step
+  // concurrent branches of a stage: 0 none; 1 fault slabs and nodes, PML
+  // slabs and shell beside the interior kernel; 2 the interior kernel
+  // alone, then the fault slabs and nodes beside the PML slabs and shell
+  // (CGFD_BRANCHES): streams and fork / join events
+  int branches = 2;
   cudaStream_t aux[3] = {};
   cudaEvent_t ev_fork[4] = {}, ev_join[4][3] = {};
   double run_ms = 0, vol_ms = 0, int_ms = 0;
@@ -178,8 +180,9 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     // branches: after the trial traction (which refreshes the stage input
     // at the split nodes), the fault slabs and nodes, the interior kernel
     // and the PML slabs / shell read the same input and write disjoint
-    // points, so they run on three streams joined before the next stage
-    const bool br = s->branches > 0;
+    // points, so they may run on separate streams joined before the next
+    // stage
+    const bool br = s->branches == 1, br2 = s->branches == 2;
     FaultArgs fargs[MAXF];
     int nfa = 0;
     for (auto &F : s->faults) {
@@ -207,7 +210,8 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       cudaStreamWaitEvent(st_fault, s->ev_fork[stage], 0);
       cudaStreamWaitEvent(st_pml, s->ev_fork[stage], 0);
     }
-    for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
+    if (!br2)
+      for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
     VolArgs v{};
     v.g = s->g; v.cur = s->w[scur]; v.pre = s->w[spre]; v.out = sout >= 0 ? s->w[sout] : nullptr; v.end = s->w[send];
     v.coef = s->coef; v.free_mat = s->free_mat;
@@ -225,6 +229,14 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       // interior box, single-direction PML slabs, generic shell
       const int kind0 = 0;
       for (int kind = kind0; kind < 5; kind++) {
+        if (kind == 1 && br2) {
+          // the interior kernel has been issued alone; the fault kernels
+          // now overlap the PML slabs and the shell
+          st_fault = s->aux[0];
+          cudaEventRecord(s->ev_fork[stage], s->stream);
+          cudaStreamWaitEvent(st_fault, s->ev_fork[stage], 0);
+          for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
+        }
         VolArgs vk = vs;
         volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind != 0 && s->pack);
         vk.ychunk = s->ychunk;
@@ -248,6 +260,9 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       cudaEventRecord(s->ev_join[stage][1], st_pml);
       cudaStreamWaitEvent(s->stream, s->ev_join[stage][0], 0);
       cudaStreamWaitEvent(s->stream, s->ev_join[stage][1], 0);
+    } else if (br2) {
+      cudaEventRecord(s->ev_join[stage][0], st_fault);
+      cudaStreamWaitEvent(s->stream, s->ev_join[stage][0], 0);
     }
     if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
   }
