@@ -279,6 +279,10 @@ __device__ __forceinline__ bool locate_interior(const VolArgs &a, int &i, int &j
   return i <= B.i1 && j <= B.j1;
 }
 
+#ifndef CGFD_PREFETCH
+#define CGFD_PREFETCH 1
+#endif
+
 // resident blocks per SM asked of the compiler, per kernel kind (register
 // budget 65536 / (256 x blocks))
 #ifndef CGFD_LB_INTERIOR
@@ -307,6 +311,16 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   }
   const long p = g.at(I, J, K);
   const long sc = g.scmp;
+#if CGFD_PREFETCH
+  if (MODE != RK_FIRST) {
+    // the RK update reads the time-n level and the accumulator last: ask
+    // L2 for their lines now, so that those reads wait on L2, not DRAM
+    const float *q[6] = { a.end + 4 * p, a.end + 4 * sc + 4 * p, a.end + 8 * sc + p,
+                          a.pre + 4 * p, a.pre + 4 * sc + 4 * p, a.pre + 8 * sc + p };
+#pragma unroll
+    for (int n = 0; n < (MODE == RK_MID ? 6 : 3); n++) asm volatile("prefetch.global.L2 [%0];" ::"l"(q[n]));
+  }
+#endif
   const Taps w = taps_at(a.cur, sc, p);
   float v0[9];
   ld9(w, 0, v0);
