@@ -106,7 +106,7 @@ struct cgfd_solver {
   long long int_points = 0, vol_points = 0;   // points one launch updates
   int it = 0;
   long long launches_per_step = 0, last_launches = 0;
-  int ychunk = 16;                      // interior kernel: y tiles per z-marching chunk
+  int ychunk = 16;                      // interior kernel: y tiles per z-marching chunk (set at upload)
   bool pack = true;                     // pack boxes at most 24 points wide (x PML slabs)
   int box_top[1][6];                    // rows under the free surface
   int box_in[1][6];                     // interior box (no PML, no surface rows)
@@ -398,6 +398,8 @@ int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
   return rc;
 }
 
+static int build_graphs(cgfd_solver *s);
+
 int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   if (!su || !out) return fail(CGFD_ERR_ARG, "null argument");
   *out = nullptr;
@@ -547,6 +549,14 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     std::memcpy(s->box_top[0], bt, sizeof bt);
     const char *pk = std::getenv("CGFD_PACK");
     if (pk && pk[0] == '0') s->pack = false;
+    // y tiles (8 rows) per interior chunk: the z window of a chunk, about 8
+    // planes of the stage input (36 B a point), should take at most ~24 MB
+    // of the 126 MB L2, which also carries the streamed arrays (measured:
+    // 1200x600x400 best at 16-24 tiles, 600x300x240 at its whole plane)
+    {
+      const long row_bytes = (long)std::max(1, ihi - ilo + 1) * 8 * 36;
+      s->ychunk = (int)std::max(4L, (24L << 20) / (8 * row_bytes));
+    }
     const char *yc = std::getenv("CGFD_INTERIOR_YCHUNK");
     if (yc && std::atoi(yc) > 0) s->ychunk = std::atoi(yc);
     s->ychunk = std::min(s->ychunk, std::max(1, (jhi - jlo + 8) / 8));
@@ -588,7 +598,47 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   }
   CK(cudaStreamSynchronize(s->stream), "set-up");
 #undef CK
+  {
+    const int rc = build_graphs(s);
+    if (rc != CGFD_OK) { destroy(s); return rc; }
+  }
   *out = s;
+  return CGFD_OK;
+}
+
+// capture step `it` (its operator pair it % 8, its level parity) into the
+// graph of the current timing mode
+static int build_graph(cgfd_solver *s, int it) {
+  cudaGraphExec_t &G = s->graph[s->timing][it % 8];
+  cudaGraph_t gr;
+  cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(e, "begin capture");
+  enqueue_step(s, it);
+  // a launch refused during capture (bad configuration) is not part of the
+  // graph and would otherwise go unnoticed
+  const cudaError_t le = cudaGetLastError();
+  e = cudaStreamEndCapture(s->stream, &gr);
+  if (le != cudaSuccess) {
+    if (e == cudaSuccess) cudaGraphDestroy(gr);
+    return cuda_fail(le, "launch");
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "end capture");
+  e = cudaGraphInstantiate(&G, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) { G = nullptr; return cuda_fail(e, "instantiate"); }
+  return CGFD_OK;
+}
+
+// the 8 step graphs of the current timing mode, built before any run so
+// that no capture or instantiation happens between the launches of a run
+static int build_graphs(cgfd_solver *s) {
+  if (!s->use_graph) return CGFD_OK;
+  for (int q = 0; q < 8; q++) {
+    const int it = s->it + q;
+    if (s->graph[s->timing][it % 8]) continue;
+    const int rc = build_graph(s, it);
+    if (rc != CGFD_OK) return rc;
+  }
   return CGFD_OK;
 }
 
@@ -629,22 +679,8 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
     if (s->use_graph) {
       cudaGraphExec_t &G = s->graph[s->timing][it % 8];
       if (!G) {
-        cudaGraph_t gr;
-        e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return cuda_fail(e, "begin capture");
-        enqueue_step(s, it);
-        // a launch refused during capture (bad configuration) is not part
-        // of the graph and would otherwise go unnoticed
-        const cudaError_t le = cudaGetLastError();
-        e = cudaStreamEndCapture(s->stream, &gr);
-        if (le != cudaSuccess) {
-          if (e == cudaSuccess) cudaGraphDestroy(gr);
-          return cuda_fail(le, "launch");
-        }
-        if (e != cudaSuccess) return cuda_fail(e, "end capture");
-        e = cudaGraphInstantiate(&G, gr, 0);
-        cudaGraphDestroy(gr);
-        if (e != cudaSuccess) { G = nullptr; return cuda_fail(e, "instantiate"); }
+        const int rc = build_graph(s, it);
+        if (rc != CGFD_OK) return rc;
       }
       e = cudaGraphLaunch(G, s->stream);
       if (e != cudaSuccess) return cuda_fail(e, "graph launch");
@@ -839,7 +875,7 @@ void cgfd_ensemble_destroy(cgfd_ensemble *e) { ensemble_free(e); }
 int cgfd_set_timing(cgfd_solver *s, int on) {
   if (!s) return fail(CGFD_ERR_ARG, "bad argument");
   s->timing = on ? 1 : 0;
-  return CGFD_OK;
+  return build_graphs(s);
 }
 
 int cgfd_last_timing(const cgfd_solver *s, double *run_ms, double *volume_ms, long long *volume_launches) {

@@ -237,7 +237,10 @@ int cgfd_last_launches(const cgfd_solver *s, long long *launches);
 
 /* 1: time every volume-stage launch with CUDA events on the solver's
  * stream (cgfd_run reads each step's events 8 steps later, so the host
- * never waits on the step in flight); 0: off (default). */
+ * never waits on the step in flight); 0: off (default).  Switching builds
+ * the step graphs of the new mode if they do not exist yet (cgfd_upload
+ * builds those of the default mode), so that no graph is captured or
+ * instantiated inside a run. */
 int cgfd_set_timing(cgfd_solver *s, int on);
 /* Device time of the last cgfd_run (events on the solver's stream at its
  * start and end) and, with timing on, the summed duration and count of its
