@@ -166,6 +166,22 @@ __device__ __forceinline__ void st9(float *w, long sc, long p, const float v[9],
       make_float4(v[4] + k * h[4], v[5] + k * h[5], v[6] + k * h[6], v[7] + k * h[7]);
   w[8 * sc + p] = v[8] + k * h[8];
 }
+// L2 prefetch of the auxiliary-field lines that pml_face reads at (I, J, K)
+template <int MODE>
+__device__ __forceinline__ void pml_prefetch(const PmlFaceDev &P, int I, int J, int K) {
+  const int li = I - P.i1, lj = J - P.j1, lk = K - P.k1;
+  if (li < 0 || li >= P.fni || lj < 0 || lj >= P.fnj || lk < 0 || lk >= P.fnk) return;
+  const long pa = li + (long)lj * P.fni + (long)lk * P.fni * P.fnj, sz = P.siz;
+  const float *lv[3] = { P.acur, MODE == RK_MID ? P.apre : nullptr, MODE != RK_FIRST ? P.aend : nullptr };
+#pragma unroll
+  for (int l = 0; l < 3; l++) {
+    if (!lv[l]) continue;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(lv[l] + 4 * pa));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(lv[l] + 4 * sz + 4 * pa));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(lv[l] + 8 * sz + pa));
+  }
+}
+
 // PML face P (normal d) at this point: add its correction to corr and
 // advance its auxiliary fields (stored like a wavefield level, grouped,
 // with P.siz points per component)
@@ -319,6 +335,14 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
                           a.pre + 4 * p, a.pre + 4 * sc + 4 * p, a.pre + 8 * sc + p };
 #pragma unroll
     for (int n = 0; n < (MODE == RK_MID ? 6 : 3); n++) asm volatile("prefetch.global.L2 [%0];" ::"l"(q[n]));
+  }
+  // likewise the auxiliary fields of the PML faces this point lies in
+  if (KIND != INTERIOR) {
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+      if (KIND >= FACE_X && f / 2 != KIND - FACE_X) continue;
+      if (a.pml[f].on) pml_prefetch<MODE>(a.pml[f], I, J, K);
+    }
   }
 #endif
   const Taps w = taps_at(a.cur, sc, p);
