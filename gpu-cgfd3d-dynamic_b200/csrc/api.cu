@@ -28,6 +28,7 @@ void launch_volume_shell(const VolArgs &a, int idir, int jdir, int kdir, int mod
 void launch_volume_face_x(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume_edge(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 int launch_fault_pre(const FaultArgs &a, cudaStream_t st);
 int launch_fault_post(const FaultArgs &a, cudaStream_t st);
 cudaError_t noalloc_scratch_address(float **p);
@@ -113,8 +114,8 @@ struct cgfd_solver {
   // boxes of each volume kernel kind: 0 interior, 1 generic shell (PML
   // edges / corners, surface rows), 2..4 slabs reached by the PML faces of
   // one direction only (x, y, z)
-  int kbox[5][12][6];
-  int nkbox[5] = {};
+  int kbox[6][12][6];
+  int nkbox[6] = {};
   std::vector<void *> allocs;
 };
 
@@ -228,7 +229,7 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     {
       // interior box, single-direction PML slabs, generic shell
       const int kind0 = 0;
-      for (int kind = kind0; kind < 5; kind++) {
+      for (int kind = kind0; kind < 6; kind++) {
         if (kind == 1 && br2) {
           // the interior kernel has been issued alone; the fault kernels
           // now overlap the PML slabs and the shell
@@ -250,7 +251,8 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
           case 1: launch_volume_shell(vk, idir, jdir, kdir, mode, st_pml); break;
           case 2: launch_volume_face_x(vk, idir, jdir, kdir, mode, st_pml); break;
           case 3: launch_volume_face_y(vk, idir, jdir, kdir, mode, st_pml); break;
-          default: launch_volume_face_z(vk, idir, jdir, kdir, mode, st_pml); break;
+          case 4: launch_volume_face_z(vk, idir, jdir, kdir, mode, st_pml); break;
+          default: launch_volume_edge(vk, idir, jdir, kdir, mode, st_pml); break;
         }
         nl += vk.nbox > 0;
       }
@@ -528,22 +530,23 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     add(3, ilo, ihi, jhi + 1, nj - 1, klo, khi);
     add(4, ilo, ihi, jlo, jhi, 0, klo - 1);
     if (!s->isfree) add(4, ilo, ihi, jlo, jhi, khi + 1, nk - 1);
-    // vertical edges, bottom ring, top ring or surface rows
-    add(1, 0, ilo - 1, 0, jlo - 1, klo, khi);
-    add(1, 0, ilo - 1, jhi + 1, nj - 1, klo, khi);
-    add(1, ihi + 1, ni - 1, 0, jlo - 1, klo, khi);
-    add(1, ihi + 1, ni - 1, jhi + 1, nj - 1, klo, khi);
-    add(1, 0, ilo - 1, 0, nj - 1, 0, klo - 1);
-    add(1, ihi + 1, ni - 1, 0, nj - 1, 0, klo - 1);
-    add(1, ilo, ihi, 0, jlo - 1, 0, klo - 1);
-    add(1, ilo, ihi, jhi + 1, nj - 1, 0, klo - 1);
+    // vertical edges, bottom ring, top ring (edge kernel); surface rows
+    // (shell kernel)
+    add(5, 0, ilo - 1, 0, jlo - 1, klo, khi);
+    add(5, 0, ilo - 1, jhi + 1, nj - 1, klo, khi);
+    add(5, ihi + 1, ni - 1, 0, jlo - 1, klo, khi);
+    add(5, ihi + 1, ni - 1, jhi + 1, nj - 1, klo, khi);
+    add(5, 0, ilo - 1, 0, nj - 1, 0, klo - 1);
+    add(5, ihi + 1, ni - 1, 0, nj - 1, 0, klo - 1);
+    add(5, ilo, ihi, 0, jlo - 1, 0, klo - 1);
+    add(5, ilo, ihi, jhi + 1, nj - 1, 0, klo - 1);
     if (s->isfree) {
       add(1, 0, ni - 1, 0, nj - 1, khi + 1, nk - 1);
     } else {
-      add(1, 0, ilo - 1, 0, nj - 1, khi + 1, nk - 1);
-      add(1, ihi + 1, ni - 1, 0, nj - 1, khi + 1, nk - 1);
-      add(1, ilo, ihi, 0, jlo - 1, khi + 1, nk - 1);
-      add(1, ilo, ihi, jhi + 1, nj - 1, khi + 1, nk - 1);
+      add(5, 0, ilo - 1, 0, nj - 1, khi + 1, nk - 1);
+      add(5, ihi + 1, ni - 1, 0, nj - 1, khi + 1, nk - 1);
+      add(5, ilo, ihi, 0, jlo - 1, khi + 1, nk - 1);
+      add(5, ilo, ihi, jhi + 1, nj - 1, khi + 1, nk - 1);
     }
     const int bt[6] = { 0, g.ni - 1, 0, g.nj - 1, s->isfree ? g.nk - 4 : g.nk, g.nk - 1 };
     std::memcpy(s->box_top[0], bt, sizeof bt);

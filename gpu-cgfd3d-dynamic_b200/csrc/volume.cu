@@ -251,9 +251,11 @@ __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float 
 }
 
 // kernel kinds: the interior box (no boundary logic), slabs that only PML
-// faces of one direction reach (x, y or z), and the generic shell (edges
-// and corners where faces overlap, rows under the free surface)
-enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4 };
+// faces of one direction reach (x, y or z), the generic shell (the rows
+// under the free surface, with any PML faces), and the PML edges and
+// corners away from the free surface (the shell's code without the
+// free-surface logic, which keeps it in registers)
+enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4, EDGE = 5 };
 
 // block -> point; boxes with a narrow x extent (PML x slabs) pack their
 // points densely instead of leaving most of a 32-wide row idle
@@ -313,9 +315,9 @@ __device__ __forceinline__ bool locate_interior(const VolArgs &a, int &i, int &j
 
 template <int ID, int JD, int KD, int MODE, int KIND>
 __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
-                                         : (KIND == SHELL ? CGFD_LB_SHELL : CGFD_LB_FACE))
+                                         : (KIND == SHELL || KIND == EDGE ? CGFD_LB_SHELL : CGFD_LB_FACE))
     k_volume(const __grid_constant__ VolArgs a) {
-  static_assert(KIND >= INTERIOR && KIND <= FACE_Z, "kernel kind");
+  static_assert(KIND >= INTERIOR && KIND <= EDGE, "kernel kind");
   const Grid &g = a.g;
   int i, j, k;
   if (KIND == INTERIOR ? !locate_interior(a, i, j, k) : !locate(a, i, j, k)) return;
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   if (KIND != INTERIOR) {
 #pragma unroll
     for (int f = 0; f < 6; f++) {
-      if (KIND >= FACE_X && f / 2 != KIND - FACE_X) continue;
+      if (KIND >= FACE_X && KIND <= FACE_Z && f / 2 != KIND - FACE_X) continue;
       if (a.pml[f].on) pml_prefetch<MODE>(a.pml[f], I, J, K);
     }
   }
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     return;
   }
 
-  if (KIND >= FACE_X) {
+  if constexpr (KIND >= FACE_X && KIND <= FACE_Z) {
     // one PML direction FD: the other two directions accumulate like the
     // interior, direction FD is kept apart for the face's correction and
     // auxiliary update
@@ -406,10 +408,10 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     return;
   }
 
-  // ---- shell: PML edges and corners, rows under the free surface ----------
+  // ---- shell and edges: PML edges and corners, rows under the free surface
   const int nk2 = g.nk + NG - 1;
-  const bool top = a.isfree && K >= nk2 - 3;
-  const bool surfrow = a.isfree && K == nk2;
+  const bool top = KIND == SHELL && a.isfree && K >= nk2 - 3;
+  const bool surfrow = KIND == SHELL && a.isfree && K == nk2;
   const long fidx = ((long)J * g.nx + I) * 9;
   float corr[9], r[9], D[9], dvx[3], dvy[3];
 #pragma unroll
@@ -531,7 +533,7 @@ void launch_kind(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaS
 
 }  // namespace
 
-// This file is compiled once per kernel kind (CGFD_VOLUME_KIND = 0..4, set
+// This file is compiled once per kernel kind (CGFD_VOLUME_KIND = 0..5, set
 // by the build) so that the 24 instantiations of each kind build in
 // parallel; unit 0 also holds the host helpers.
 #ifndef CGFD_VOLUME_KIND
@@ -581,9 +583,13 @@ void launch_volume_face_x(const VolArgs &a, int idir, int jdir, int kdir, int mo
 void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
   launch_kind<FACE_Y>(a, idir, jdir, kdir, mode, st);
 }
-#else
+#elif CGFD_VOLUME_KIND == 4
 void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
   launch_kind<FACE_Z>(a, idir, jdir, kdir, mode, st);
+}
+#else
+void launch_volume_edge(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<EDGE>(a, idir, jdir, kdir, mode, st);
 }
 #endif
 
