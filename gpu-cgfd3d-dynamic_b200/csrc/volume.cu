@@ -41,15 +41,18 @@ constexpr int BX = 32, BY = 8;
 
 
 // conservative traction J * (e . sigma_row) at point q for metric row d
-// (0: xi, 1: eta, 2: zeta) and stress row r (0: xx,xy,xz; 1: xy,yy,yz;
-// 2: xz,yz,zz)
-__device__ __forceinline__ float ctrac(const Grid &g, const float *__restrict__ w, const float *__restrict__ cf,
-                                       long q, int d, int r) {
-  const int c0 = r == 0 ? TXX : (r == 1 ? TXY : TXZ);
-  const int c1 = r == 0 ? TXY : (r == 1 ? TYY : TYZ);
-  const int c2 = r == 0 ? TXZ : (r == 1 ? TYZ : TZZ);
+// (0: xi, 1: eta, 2: zeta), all three stress rows (xx,xy,xz), (xy,yy,yz),
+// (xz,yz,zz)
+__device__ __forceinline__ void ctrac3(const Grid &g, const float *__restrict__ w, const float *__restrict__ cf,
+                                       long q, int d, float t[3]) {
   const float4 e = coef_row(cf, g.scmp, d, q);
-  return coef_jac(cf, q) * (e.x * __ldg(w + g.w(c0, q)) + e.y * __ldg(w + g.w(c1, q)) + e.z * __ldg(w + g.w(c2, q)));
+  const float J = coef_jac(cf, q);
+  const float sxx = __ldg(w + g.w(TXX, q)), sxy = __ldg(w + g.w(TXY, q));
+  const float4 s4 = __ldg(reinterpret_cast<const float4 *>(w + 4 * g.scmp) + q);   // Tyy Tzz Tyz Txz
+  const float syy = s4.x, szz = s4.y, syz = s4.z, sxz = s4.w;
+  t[0] = J * (e.x * sxx + e.y * sxy + e.z * sxz);
+  t[1] = J * (e.x * sxy + e.y * syy + e.z * syz);
+  t[2] = J * (e.x * sxz + e.y * syz + e.z * szz);
 }
 
 // the point's three groups within one level
@@ -475,27 +478,36 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     const float *cur = a.cur;
     const long sy = g.sy;
     const float sj = slw / coef_jac(a.coef, p);
-#pragma unroll 1
-    for (int rr = 0; rr < 3; rr++) {
-      float dx = 0.f, dy = 0.f, dzz = 0.f;
+    // per tap the three traction rows at once; each row's sum over the
+    // taps keeps the order of the coefficient table
+    float dx[3] = { 0.f, 0.f, 0.f }, dy[3] = { 0.f, 0.f, 0.f }, dzz[3] = { 0.f, 0.f, 0.f };
+    float t[3];
 #pragma unroll
-      for (int n = 0; n < 5; n++) dx += wdrp<ID>(n) * ctrac(g, cur, a.coef, p + (ID ? n - 1 : n - 3), 0, rr);
+    for (int n = 0; n < 5; n++) {
+      ctrac3(g, cur, a.coef, p + (ID ? n - 1 : n - 3), 0, t);
 #pragma unroll
-      for (int n = 0; n < 5; n++) dy += wdrp<JD>(n) * ctrac(g, cur, a.coef, p + (JD ? n - 1 : n - 3) * sy, 1, rr);
-#pragma unroll
-      for (int n = 0; n < 5; n++) {
-        const int kk = K + (KD ? n - 1 : n - 3);
-        float v = 0.f;
-        if (kk < nk2) v = ctrac(g, cur, a.coef, g.at(I, J, kk), 2, rr);
-        else if (kk > nk2) v = -ctrac(g, cur, a.coef, g.at(I, J, 2 * nk2 - kk), 2, rr);
-        dzz += wdrp<KD>(n) * v;
-      }
-      // select instead of h[VX + rr]: a runtime index would move h to the stack
-      const float hv = (dx + dy + dzz) * sj;
-      h[VX] = rr == 0 ? hv : h[VX];
-      h[VY] = rr == 1 ? hv : h[VY];
-      h[VZ] = rr == 2 ? hv : h[VZ];
+      for (int rr = 0; rr < 3; rr++) dx[rr] += wdrp<ID>(n) * t[rr];
     }
+#pragma unroll
+    for (int n = 0; n < 5; n++) {
+      ctrac3(g, cur, a.coef, p + (JD ? n - 1 : n - 3) * sy, 1, t);
+#pragma unroll
+      for (int rr = 0; rr < 3; rr++) dy[rr] += wdrp<JD>(n) * t[rr];
+    }
+#pragma unroll
+    for (int n = 0; n < 5; n++) {
+      const int kk = K + (KD ? n - 1 : n - 3);
+      if (kk == nk2) {
+        t[0] = t[1] = t[2] = 0.f;
+      } else {
+        ctrac3(g, cur, a.coef, g.at(I, J, kk < nk2 ? kk : 2 * nk2 - kk), 2, t);
+        if (kk > nk2) { t[0] = -t[0]; t[1] = -t[1]; t[2] = -t[2]; }
+      }
+#pragma unroll
+      for (int rr = 0; rr < 3; rr++) dzz[rr] += wdrp<KD>(n) * t[rr];
+    }
+#pragma unroll
+    for (int rr = 0; rr < 3; rr++) h[VX + rr] = (dx[rr] + dy[rr] + dzz[rr]) * sj;
   }
 #pragma unroll
   for (int c = 0; c < 9; c++) h[c] += corr[c];
