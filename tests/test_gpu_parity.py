@@ -191,3 +191,25 @@ def test_sponge_with_pml_rejected(cgfd_lib):
     p = dataclasses.replace(inputs.small_planar(nt=10), ablexp_layers=((4, 4), (0, 0), (0, 0)))
     with pytest.raises(Exception, match="ERR_ARG"):
         Solver(p)
+
+
+def test_error_against_fp64(cgfd_lib, oracle_built):
+    """Error of the float32 CUDA path against the FP64 build of the same
+    scheme (the double-precision oracle), beside the error of the float32
+    oracle, which does the reference's float arithmetic: the CUDA path may
+    differ from FP64 only as much as float32 arithmetic of the scheme does."""
+    nt = 80
+    p = inputs.small_planar(nt=nt)
+    g, o32, o64 = Solver(p), OracleSolver(p), OracleSolver(p, double=True)
+    for s in (g, o32, o64):
+        s.run(nt)
+    errs = {}
+    for f in ("Vs", "Slip", "Peak_vs", "Ts1"):
+        ref = o64.fault(f)
+        errs[f] = (rel_l2(g.fault(f), ref), rel_l2(o32.fault(f), ref))
+    ref = o64.stations()[:, :3]
+    errs["stations"] = (rel_l2(g.stations()[:, :3], ref), rel_l2(o32.stations()[:, :3], ref))
+    print("rel-L2 vs FP64 (cuda, float oracle):", {k: (f"{a:.2e}", f"{b:.2e}") for k, (a, b) in errs.items()})
+    for k, (gpu, f32) in errs.items():
+        assert gpu < TOL, k
+        assert gpu <= 4.0 * f32 + 1e-7, (k, gpu, f32)
