@@ -303,6 +303,11 @@ __device__ __forceinline__ bool locate_interior(const VolArgs &a, int &i, int &j
 #ifndef CGFD_PREFETCH
 #define CGFD_PREFETCH 1
 #endif
+// interior kernel: z rows ahead whose DRAM misses each thread prefetches
+// (0: none)
+#ifndef CGFD_AHEAD
+#define CGFD_AHEAD 1
+#endif
 
 // resident blocks per SM asked of the compiler, per kernel kind (register
 // budget 65536 / (256 x blocks))
@@ -341,6 +346,25 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
 #pragma unroll
     for (int n = 0; n < (MODE == RK_MID ? 6 : 3); n++) asm volatile("prefetch.global.L2 [%0];" ::"l"(q[n]));
   }
+#if CGFD_AHEAD > 0
+  if (KIND == INTERIOR) {
+    // the DRAM misses of the block CGFD_AHEAD z rows up: the newest stencil
+    // plane of the stage input and its coefficients (that block runs soon
+    // after this one: blocks march up z within a y chunk)
+    const int kn = K + CGFD_AHEAD + (KD ? 3 : 1), kc = K + CGFD_AHEAD;
+    if (kn < g.nz) {
+      const long q = p + (long)(kn - K) * g.sz;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a.cur + 4 * q));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a.cur + 4 * sc + 4 * q));
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(a.cur + 8 * sc + q));
+    }
+    if (kc < g.nz) {
+      const long q = p + (long)CGFD_AHEAD * g.sz;
+#pragma unroll
+      for (int d = 0; d < 3; d++) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.coef + sc + 4 * (d * sc + q)));
+    }
+  }
+#endif
   // likewise the auxiliary fields of the PML faces this point lies in
   if (KIND != INTERIOR) {
 #pragma unroll
