@@ -353,35 +353,12 @@ int cgfd_setup_coords(const cgfd_setup *su, float *x, float *y, float *z) {
 int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes) {
   if (!su || !bytes) return fail(CGFD_ERR_ARG, "bad argument");
   const HostSetup &H = su->H;
-  unsigned long long n = (H.metric.size() + H.media.size() + H.free_mat.size()) * 4ull;
+  unsigned long long n = (H.coef.size() + H.free_mat.size()) * 4ull;
   for (int d = 0; d < 3; d++) for (int q = 0; q < 2; q++) n += 3ull * (H.pml[d][q].A.size()) * 4;
   for (auto &F : H.faults) n += F.flag.size() + (F.mat.size() + F.fmat.size() + F.scal.size() + F.out.size()) * 4ull;
   n += H.sta_idx.size() * sizeof(long) + (H.sta_w.size() + H.fsta_w.size()) * 4ull + (H.fsta_fid.size() + H.fsta_idx.size()) * 4ull;
   *bytes = n;
   return CGFD_OK;
-}
-
-// the host metric [10][scmp] and medium [3][scmp] as the device block of
-// coef_row / coef_jac: the Jacobian plane, then per direction d the groups
-// (e_d.x, e_d.y, e_d.z, medium d), packed and copied in chunks
-static cudaError_t upload_coef(cgfd_solver *s, const HostSetup &H) {
-  const size_t sc = s->g.scmp;
-  cudaError_t e = cudaMemcpyAsync(s->coef, H.metric.data() + (size_t)MJAC * sc, sc * 4, cudaMemcpyHostToDevice, s->stream);
-  const size_t chunk = (size_t)1 << 22;
-  std::vector<float> buf(4 * std::min(chunk, sc));
-  for (int d = 0; d < 3 && e == cudaSuccess; d++) {
-    const float *ex = H.metric.data() + (size_t)(MXIX + 3 * d) * sc, *m = H.media.data() + (size_t)d * sc;
-    for (size_t q0 = 0; q0 < sc && e == cudaSuccess; q0 += chunk) {
-      const size_t n = std::min(chunk, sc - q0);
-      for (size_t q = 0; q < n; q++) {
-        buf[4 * q] = ex[q0 + q]; buf[4 * q + 1] = ex[sc + q0 + q]; buf[4 * q + 2] = ex[2 * sc + q0 + q];
-        buf[4 * q + 3] = m[q0 + q];
-      }
-      e = cudaMemcpyAsync(s->coef + sc + 4 * (d * sc + q0), buf.data(), n * 16, cudaMemcpyHostToDevice, s->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    }
-  }
-  return e;
 }
 
 int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
@@ -423,7 +400,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
   CK(dalloc(s, &s->coef, 13 * (size_t)g.scmp), "metric");
   CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
-  CK(upload_coef(s, H), "copy metric");
+  CK(cudaMemcpyAsync(s->coef, H.coef.data(), H.coef.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy metric");
   CK(cudaMemcpyAsync(s->free_mat, H.free_mat.data(), H.free_mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy free");
   if (H.abl_nblk > 0) {
     CK(dalloc(s, &s->abl_E, (size_t)g.nx + g.ny + g.nz), "sponge");

@@ -234,14 +234,26 @@ int build_setup(const cgfd_config *c, HostSetup &S, std::string &msg) {
     msg = b; return CGFD_ERR_DT;
   }
 
-  // ---- copy metric and medium into the padded device layout --------------
-  S.metric.assign((size_t)10 * g.scmp, 0.f);
-  S.media.assign((size_t)3 * g.scmp, 0.f);
-  for (int k = 0; k < nz; k++) for (int j = 0; j < ny; j++) for (int i = 0; i < nx; i++) {
-    size_t p = U(i,j,k), d = (size_t)g.at(i,j,k);
-    for (int q = 0; q < 10; q++) S.metric[(size_t)q*g.scmp + d] = Mp[q][p];
-    S.media[d] = lam[p]; S.media[g.scmp + d] = mu[p];
-    S.media[2*g.scmp + d] = rho[p] > 1e-10f ? (float)(1.0 / rho[p]) : 0.f;
+  // ---- metric and medium in the padded device layout (coef_row /
+  //      coef_jac of common.h): the Jacobian plane, then per direction d
+  //      the groups (e_d.x, e_d.y, e_d.z, lambda | mu | 1/rho) ------------
+  S.coef.assign((size_t)13 * g.scmp, 0.f);
+  {
+    const size_t sc = g.scmp;
+    float *jac = S.coef.data(), *grp = S.coef.data() + sc;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          const size_t p = U(i,j,k), d = (size_t)g.at(i,j,k);
+          const float med[3] = { lam[p], mu[p], rho[p] > 1e-10f ? (float)(1.0 / rho[p]) : 0.f };
+          jac[d] = Mp[MJAC][p];
+          for (int r = 0; r < 3; r++) {
+            float *o = grp + 4 * (r * sc + d);
+            o[0] = Mp[MXIX + 3 * r][p]; o[1] = Mp[MXIX + 3 * r + 1][p]; o[2] = Mp[MXIX + 3 * r + 2][p];
+            o[3] = med[r];
+          }
+        }
   }
 
   // ---- CFS-PML (bdry_pml_set, bdry_t.cu:80-251 and 292-440) --------------

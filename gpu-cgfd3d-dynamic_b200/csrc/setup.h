@@ -33,8 +33,10 @@ struct HostSetup {
   Grid g;
   float dt = 0.f, dtmax = 0.f;
   int imethod = 2, isfree = 0;
-  std::vector<float> metric;      // [10][scmp]
-  std::vector<float> media;       // [3][scmp]: lambda, mu, 1/rho
+  // metric and medium as the device reads them: [scmp] Jacobian, then
+  // [3][scmp][4] (metric row d, medium value d) with the medium values
+  // lambda, mu, 1/rho
+  std::vector<float> coef;
   std::vector<float> free_mat;    // [2][ny][nx][9]: matVx2Vz, matVy2Vz at the surface
   std::vector<float> coords;      // [3][nk][nj][ni]: x, y, z of the interior grid points
   PmlHost pml[3][2];
