@@ -121,6 +121,13 @@ struct cgfd_solver {
 
 struct cgfd_setup {
   cgfd::HostSetup H;
+  // the packed metric and medium (H.coef) moved to page-locked memory when
+  // a device is present, so that cgfd_upload copies it at full link rate
+  float *coef_pinned = nullptr;
+  size_t coef_n = 0;
+  const float *coef() const { return coef_pinned ? coef_pinned : H.coef.data(); }
+  size_t coef_size() const { return coef_pinned ? coef_n : H.coef.size(); }
+  ~cgfd_setup() { if (coef_pinned) cudaFreeHost(coef_pinned); }
 };
 
 namespace {
@@ -319,6 +326,18 @@ int cgfd_prepare(const cgfd_config *cfg, cgfd_setup **out) {
   std::string msg;
   int rc = build_setup(cfg, su->H, msg);
   if (rc != CGFD_OK) { delete su; return fail(rc, msg); }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0) {
+    float *pc = nullptr;
+    const size_t n = su->H.coef.size();
+    if (cudaMallocHost((void **)&pc, n * sizeof(float)) == cudaSuccess) {
+      std::memcpy(pc, su->H.coef.data(), n * sizeof(float));
+      su->coef_pinned = pc;
+      su->coef_n = n;
+      std::vector<float>().swap(su->H.coef);
+    }
+  }
+  cudaGetLastError();   // no device, or no page-locked memory: keep the vector
   *out = su;
   return CGFD_OK;
 }
@@ -353,7 +372,7 @@ int cgfd_setup_coords(const cgfd_setup *su, float *x, float *y, float *z) {
 int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes) {
   if (!su || !bytes) return fail(CGFD_ERR_ARG, "bad argument");
   const HostSetup &H = su->H;
-  unsigned long long n = (H.coef.size() + H.free_mat.size()) * 4ull;
+  unsigned long long n = (su->coef_size() + H.free_mat.size()) * 4ull;
   for (int d = 0; d < 3; d++) for (int q = 0; q < 2; q++) n += 3ull * (H.pml[d][q].A.size()) * 4;
   for (auto &F : H.faults) n += F.flag.size() + (F.mat.size() + F.fmat.size() + F.scal.size() + F.out.size()) * 4ull;
   n += H.sta_idx.size() * sizeof(long) + (H.sta_w.size() + H.fsta_w.size()) * 4ull + (H.fsta_fid.size() + H.fsta_idx.size()) * 4ull;
@@ -400,7 +419,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
   CK(dalloc(s, &s->coef, 13 * (size_t)g.scmp), "metric");
   CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
-  CK(cudaMemcpyAsync(s->coef, H.coef.data(), H.coef.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy metric");
+  CK(cudaMemcpyAsync(s->coef, su->coef(), su->coef_size() * 4, cudaMemcpyHostToDevice, s->stream), "copy metric");
   CK(cudaMemcpyAsync(s->free_mat, H.free_mat.data(), H.free_mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy free");
   if (H.abl_nblk > 0) {
     CK(dalloc(s, &s->abl_E, (size_t)g.nx + g.ny + g.nz), "sponge");
