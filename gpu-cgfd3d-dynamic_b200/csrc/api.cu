@@ -101,7 +101,10 @@ struct cgfd_solver {
   // (CGFD_BRANCHES): streams and fork / join events
   int branches = 2;
   cudaStream_t aux[3] = {};
-  cudaEvent_t ev_fork[4] = {}, ev_join[4][3] = {};
+  cudaEvent_t ev_fork[4] = {}, ev_join[4][3] = {}, ev_pre[4] = {};
+  // the next stage's first fault kernels may overlap this stage's PML slab
+  // and edge kernels (no fault neighbourhood meets their boxes)
+  bool pre_early = false;
   double run_ms = 0, vol_ms = 0, int_ms = 0;
   long long vol_launches = 0, int_launches = 0;
   long long int_points = 0, vol_points = 0;   // points one launch updates
@@ -158,6 +161,7 @@ void destroy(cgfd_solver *s) {
   }
   for (int a = 0; a < 4; a++) {
     if (s->ev_fork[a]) cudaEventDestroy(s->ev_fork[a]);
+    if (s->ev_pre[a]) cudaEventDestroy(s->ev_pre[a]);
     for (int b = 0; b < 3; b++) if (s->ev_join[a][b]) cudaEventDestroy(s->ev_join[a][b]);
   }
   for (int q = 0; q < 3; q++) if (s->aux[q]) cudaStreamDestroy(s->aux[q]);
@@ -177,7 +181,8 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
   sa.g = s->g; sa.st = s->st; sa.w = s->w[slot(LP, it)]; sa.ns = (long)s->g.ny * s->g.nz; sa.ctl = s->ctl;
   for (size_t f = 0; f < s->faults.size(); f++) sa.fout[f] = s->faults[f].out;
   if ((s->st.n + s->st.nf) > 0 && s->st.max_rec > 0) { launch_record(sa, s->stream); nl++; }
-  for (int stage = 0; stage < 4; stage++) {
+  // the fault kernels' arguments of one stage
+  auto stage_fargs = [&](int stage, FaultArgs *fa) {
     const int idir = (kPairs[ip][0] + stage) % 2, jdir = (kPairs[ip][1] + stage) % 2, kdir = (kPairs[ip][2] + stage) % 2;
     const int mode = stage == 0 ? RK_FIRST : (stage == 3 ? RK_LAST : RK_MID);
     const int Lcur = stage == 0 ? LP : (stage == 2 ? LB : LA);
@@ -185,16 +190,9 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     const float ca = stage < 3 ? kRkA[stage] * s->dt : 0.f, cb = kRkB[stage] * s->dt;
     const int scur = slot(Lcur, it), spre = slot(LP, it), send = slot(LE, it);
     const int sout = Lout >= 0 ? slot(Lout, it) : -1;
-    // branches: after the trial traction (which refreshes the stage input
-    // at the split nodes), the fault slabs and nodes, the interior kernel
-    // and the PML slabs / shell read the same input and write disjoint
-    // points, so they may run on separate streams joined before the next
-    // stage
-    const bool br = s->branches == 1, br2 = s->branches == 2;
-    FaultArgs fargs[MAXF];
-    int nfa = 0;
+    int n = 0;
     for (auto &F : s->faults) {
-      FaultArgs &a = fargs[nfa++];
+      FaultArgs &a = fa[n++];
       a = FaultArgs{};
       a.g = s->g; a.F = F.d;
       a.wcur = s->w[scur]; a.wpre = s->w[spre]; a.wout = sout >= 0 ? s->w[sout] : nullptr; a.wend = s->w[send];
@@ -205,8 +203,42 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       a.isfree = s->isfree; a.imethod = s->imethod;
       a.j0 = F.j0; a.k0 = F.k0; a.nj = F.nj; a.nk = F.nk; a.ctl = s->ctl;
       a.trac = trac ? trac : F.trac; a.tj0 = F.j0 + NG - 3; a.tk0 = F.k0 + NG - 3; a.tnj = F.nj + 6; a.tnk = F.nk + 6;
-      nl += launch_fault_pre(a, s->stream);
+      if (F.nj > 0 && F.nk > 0) {
+        a.wj0 = std::max(0, F.j0 - 3); a.wk0 = std::max(0, F.k0 - 3);
+        a.wnj = std::min(s->g.nj - 1, F.j0 + F.nj + 2) - a.wj0 + 1;
+        a.wnk = std::min(s->g.nk - 1, F.k0 + F.nk + 2) - a.wk0 + 1;
+      } else {
+        a.wj0 = 0; a.wk0 = 0; a.wnj = s->g.nj; a.wnk = s->g.nk;
+      }
     }
+    return n;
+  };
+  // branches: after the trial traction (which refreshes the stage input
+  // at the split nodes), the fault slabs and nodes, the interior kernel
+  // and the PML slabs / shell read the same input and write disjoint
+  // points, so they may run on separate streams joined before the next
+  // stage.  With pre_early, the next stage's first fault kernels (which
+  // read only the fault's neighbourhood, away from every PML slab and
+  // edge box) start on the fault stream once this stage's interior,
+  // surface-row and fault kernels are done, beside its PML and edge kernels.
+  const bool br = s->branches == 1, br2 = s->branches == 2;
+  const bool early = br2 && s->pre_early;
+  FaultArgs fargs[MAXF], fnext[MAXF];
+  const int nfa = stage_fargs(0, fargs);
+  for (int stage = 0; stage < 4; stage++) {
+    const int idir = (kPairs[ip][0] + stage) % 2, jdir = (kPairs[ip][1] + stage) % 2, kdir = (kPairs[ip][2] + stage) % 2;
+    const int mode = stage == 0 ? RK_FIRST : (stage == 3 ? RK_LAST : RK_MID);
+    const int Lcur = stage == 0 ? LP : (stage == 2 ? LB : LA);
+    const int Lout = stage == 0 ? LA : (stage == 1 ? LB : (stage == 2 ? LA : -1));
+    const float ca = stage < 3 ? kRkA[stage] * s->dt : 0.f, cb = kRkB[stage] * s->dt;
+    const int scur = slot(Lcur, it), spre = slot(LP, it), send = slot(LE, it);
+    const int sout = Lout >= 0 ? slot(Lout, it) : -1;
+    if (stage > 0) {
+      if (early) std::memcpy(fargs, fnext, sizeof(FaultArgs) * nfa);
+      else stage_fargs(stage, fargs);
+    }
+    if (!(early && stage > 0))
+      for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fargs[f], s->stream);
     // external event nodes when captured, so that the events really fire
     // on every graph replay; the stage interval spans the fork to the join
     if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
@@ -244,6 +276,14 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
           cudaEventRecord(s->ev_fork[stage], s->stream);
           cudaStreamWaitEvent(st_fault, s->ev_fork[stage], 0);
           for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
+        }
+        if (kind == 2 && early && stage < 3) {
+          // the surface rows are issued: the next stage's input is complete
+          // in the fault's neighbourhood once they and the fault kernels end
+          cudaEventRecord(s->ev_pre[stage], s->stream);
+          cudaStreamWaitEvent(st_fault, s->ev_pre[stage], 0);
+          stage_fargs(stage + 1, fnext);
+          for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fnext[f], st_fault);
         }
         VolArgs vk = vs;
         volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind != 0 && s->pack);
@@ -546,6 +586,23 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     }
     const int bt[6] = { 0, g.ni - 1, 0, g.nj - 1, s->isfree ? g.nk - 4 : g.nk, g.nk - 1 };
     std::memcpy(s->box_top[0], bt, sizeof bt);
+    // a stage's first fault kernels read its input at i0-6..i0+6 over the
+    // split box grown by 3 nodes: when that region meets no PML slab or edge
+    // box for any fault, they may start before those kernels of the
+    // previous stage end
+    s->pre_early = !s->faults.empty();
+    for (auto &F : s->faults) {
+      if (F.nj <= 0 || F.nk <= 0) { s->pre_early = false; break; }
+      const int r[6] = { F.d.i0 - NG - 6, F.d.i0 - NG + 6, F.j0 - 3, F.j0 + F.nj + 2, F.k0 - 3, F.k0 + F.nk + 2 };
+      for (int kind = 2; kind < 6; kind++)
+        for (int b = 0; b < s->nkbox[kind]; b++) {
+          const int *B = s->kbox[kind][b];
+          if (B[0] <= r[1] && r[0] <= B[1] && B[2] <= r[3] && r[2] <= B[3] && B[4] <= r[5] && r[4] <= B[5])
+            s->pre_early = false;
+        }
+    }
+    const char *pe = std::getenv("CGFD_PRE_EARLY");
+    if (pe && pe[0] == '0') s->pre_early = false;
     const char *pk = std::getenv("CGFD_PACK");
     if (pk && pk[0] == '0') s->pack = false;
     // y tiles (8 rows) per interior chunk: the z window of a chunk, about 8
@@ -592,6 +649,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     for (int q = 0; q < 3; q++) CK(cudaStreamCreateWithFlags(&s->aux[q], cudaStreamNonBlocking), "stream");
     for (int a = 0; a < 4; a++) {
       CK(cudaEventCreateWithFlags(&s->ev_fork[a], cudaEventDisableTiming), "event");
+      CK(cudaEventCreateWithFlags(&s->ev_pre[a], cudaEventDisableTiming), "event");
       for (int b = 0; b < 3; b++) CK(cudaEventCreateWithFlags(&s->ev_join[a][b], cudaEventDisableTiming), "event");
     }
   }

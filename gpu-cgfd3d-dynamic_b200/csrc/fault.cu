@@ -140,9 +140,9 @@ __device__ void split_to_volume(const Grid &g, const float *__restrict__ cf, lon
 // ---------------------------------------------------------------------------
 __global__ void k_fault_weld(const FaultArgs a) {
   const Grid &g = a.g;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y * blockDim.y + threadIdx.y;
-  if (j >= g.nj || k >= g.nk) return;
+  const int j = a.wj0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = a.wk0 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= a.wj0 + a.wnj || k >= a.wk0 + a.wnk) return;
   const int J = j + NG, K = k + NG;
   const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny;
   if (a.F.flag[nd] & FL_SPLIT) return;
@@ -721,7 +721,7 @@ __global__ void k_advance(Ctl *c, int max_rec) {
 // kernels); returns the number of launches
 int launch_fault_pre(const FaultArgs &a, cudaStream_t st) {
   {
-    dim3 blk(32, 4), grd((a.g.nj + 31) / 32, (a.g.nk + 3) / 4);
+    dim3 blk(32, 4), grd((a.wnj + 31) / 32, (a.wnk + 3) / 4);
     k_fault_weld<<<grd, blk, 0, st>>>(a);
   }
   if (a.nj <= 0 || a.nk <= 0) return 1;

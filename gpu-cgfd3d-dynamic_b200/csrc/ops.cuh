@@ -98,6 +98,9 @@ struct FaultArgs {
   float ca, cb, rkb, dt;
   int isfree, imethod;
   int j0, k0, nj, nk;          // launch box of split nodes (interior indices)
+  // welded nodes whose fault fields a stage reads (the split box grown by
+  // the 3-node stencil reach, or the whole plane without split nodes)
+  int wj0, wk0, wnj, wnk;
   Ctl *ctl;
   // tractions J e_a . sigma of the stage input at x = i0-6..i0-1, i0+1..i0+6
   // over the split box grown by 3 nodes in j and k: [12][9][tnk][tnj],

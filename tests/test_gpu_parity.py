@@ -213,3 +213,30 @@ def test_error_against_fp64(cgfd_lib, oracle_built):
     for k, (gpu, f32) in errs.items():
         assert gpu < TOL, k
         assert gpu <= 4.0 * f32 + 1e-7, (k, gpu, f32)
+
+
+def test_early_fault_kernels(cgfd_lib, oracle_built, monkeypatch):
+    """A fault whose neighbourhood (i0 +- 6, split box + 3 nodes) stays clear of
+    every PML slab and edge box: there a stage's first fault kernels start
+    beside the previous stage's PML kernels.  The schedule changes no
+    arithmetic, so the result equals the serial schedule's bit for bit, and
+    the oracle's within the tolerance."""
+    nt, L, margin = 60, 5, 10
+    p = inputs.tpv_planar(ni=40, nj=80, nk=40, fault_x_index=21, fault_grid=[25, 56, 15, 40], nuc_half=3,
+                          pml=L, nt=nt, nsta=4, margin=margin)
+    i0 = p.fault_x_index[0] - 1
+    # PML slabs and edges occupy the outer L + 1 nodes of x, y and the bottom
+    assert i0 - 6 > L and i0 + 6 < p.ni - 1 - L
+    assert margin - 3 > L and p.nj - 1 - margin + 3 < p.nj - 1 - L and margin - 3 > L
+    g_early = Solver(p)
+    monkeypatch.setenv("CGFD_PRE_EARLY", "0")
+    g_serial = Solver(p)
+    o = OracleSolver(p)
+    for s in (g_early, g_serial, o):
+        s.run(nt)
+    assert o.fault("Vs").max() > 0.1
+    for f in ("Vs", "Slip", "Tn", "Ts1"):
+        assert np.array_equal(g_early.fault(f), g_serial.fault(f)), f
+        assert rel_l2(g_early.fault(f), o.fault(f)) < TOL, f
+    for c in range(9):
+        assert np.array_equal(g_early.wavefield(c), g_serial.wavefield(c)), WAVE_COMPONENTS[c]
