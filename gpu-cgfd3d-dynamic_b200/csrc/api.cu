@@ -10,7 +10,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -438,6 +441,66 @@ int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
 
 static int build_graphs(cgfd_solver *s);
 
+// Autotuner of the interior kernel's y chunk (the number of 8-row tiles whose
+// blocks march up z together, which sets how much of L2 the stencil planes
+// take): the first stage's interior launch is timed for a few chunk sizes
+// on the solver's state at upload, which is all zero, so the launches write
+// zeros where zeros are and change nothing.  The fastest size is kept per
+// device and interior box, so later solvers of the same shape reuse it.
+static std::mutex g_tune_mu;
+static std::map<std::array<int, 4>, int> g_tune;
+
+static cudaError_t tune_ychunk(cgfd_solver *s) {
+  if (s->nkbox[0] == 0) return cudaSuccess;
+  const int *B = s->kbox[0][0];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const std::array<int, 4> key = { dev, B[1] - B[0] + 1, B[3] - B[2] + 1, B[5] - B[4] + 1 };
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto f = g_tune.find(key);
+    if (f != g_tune.end()) { s->ychunk = f->second; return cudaSuccess; }
+  }
+  const int ntiles = (key[2] + 7) / 8, ip = s->it % 8, it = s->it;
+  VolArgs v{};
+  v.g = s->g; v.cur = s->w[slot(LP, it)]; v.pre = v.cur; v.out = s->w[slot(LA, it)]; v.end = s->w[slot(LE, it)];
+  v.coef = s->coef; v.free_mat = s->free_mat;
+  v.ca = kRkA[0] * s->dt; v.cb = kRkB[0] * s->dt; v.isfree = s->isfree;
+  v.nfault = (int)s->faults.size();
+  for (size_t f = 0; f < s->faults.size(); f++) { v.fi0[f] = s->faults[f].d.i0; v.fflag[f] = s->faults[f].flag; }
+  volume_boxes(v, s->kbox[0], s->nkbox[0], false);
+  cudaEvent_t t0, t1;
+  if ((e = cudaEventCreate(&t0)) != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&t1)) != cudaSuccess) { cudaEventDestroy(t0); return e; }
+  int best = s->ychunk;
+  float best_ms = 1e30f;
+  std::vector<int> cand;
+  for (int c : { 8, 16, 32, 64, ntiles }) {
+    c = std::max(1, std::min(c, ntiles));
+    if (std::find(cand.begin(), cand.end(), c) == cand.end()) cand.push_back(c);
+  }
+  for (int c : cand) {
+    v.ychunk = c;
+    launch_volume_interior(v, kPairs[ip][0], kPairs[ip][1], kPairs[ip][2], RK_FIRST, s->stream);
+    cudaEventRecord(t0, s->stream);
+    for (int r = 0; r < 2; r++) launch_volume_interior(v, kPairs[ip][0], kPairs[ip][1], kPairs[ip][2], RK_FIRST, s->stream);
+    cudaEventRecord(t1, s->stream);
+    if ((e = cudaEventSynchronize(t1)) != cudaSuccess) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    if (ms < best_ms) { best_ms = ms; best = c; }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  s->ychunk = best;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  return cudaSuccess;
+}
+
 int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   if (!su || !out) return fail(CGFD_ERR_ARG, "null argument");
   *out = nullptr;
@@ -654,6 +717,10 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     }
   }
   CK(cudaStreamSynchronize(s->stream), "set-up");
+  {
+    const char *tn = std::getenv("CGFD_TUNE");
+    if (!std::getenv("CGFD_INTERIOR_YCHUNK") && !(tn && tn[0] == '0')) CK(tune_ychunk(s), "tuning");
+  }
 #undef CK
   {
     const int rc = build_graphs(s);

@@ -240,3 +240,17 @@ def test_early_fault_kernels(cgfd_lib, oracle_built, monkeypatch):
         assert rel_l2(g_early.fault(f), o.fault(f)) < TOL, f
     for c in range(9):
         assert np.array_equal(g_early.wavefield(c), g_serial.wavefield(c)), WAVE_COMPONENTS[c]
+
+
+def test_interior_chunk_choice_changes_nothing(cgfd_lib, monkeypatch):
+    """The autotuned y chunk of the interior kernel and a fixed small one give
+    the same result bit for bit (the chunk only orders the blocks)."""
+    p = inputs.small_planar(nt=12)
+    g1 = Solver(p)
+    monkeypatch.setenv("CGFD_INTERIOR_YCHUNK", "1")
+    g2 = Solver(p)
+    g1.run(12)
+    g2.run(12)
+    assert np.array_equal(g1.fault("Vs"), g2.fault("Vs"))
+    for c in range(9):
+        assert np.array_equal(g1.wavefield(c), g2.wavefield(c)), WAVE_COMPONENTS[c]
