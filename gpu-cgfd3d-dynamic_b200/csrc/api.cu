@@ -37,6 +37,7 @@ int launch_fault_post(const FaultArgs &a, cudaStream_t st);
 cudaError_t noalloc_scratch_address(float **p);
 void launch_record(const StationArgs &a, cudaStream_t st);
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
+void launch_fault_gather(const float *out, float *dst, int nf, const Grid &g, cudaStream_t st);
 int launch_sponge(const SpongeArgs &a, cudaStream_t st);
 int launch_surface_peaks(const PeakArgs &a, cudaStream_t st);
 }  // namespace cgfd
@@ -63,6 +64,7 @@ struct FaultState {
   uint8_t *flag = nullptr;
   float *mat = nullptr, *fmat = nullptr, *scal = nullptr, *out = nullptr;
   float *trac = nullptr;                // traction scratch of the split box
+  float *gather = nullptr;              // output fields at interior nodes, [11][nk][nj]
 };
 
 struct PmlState {
@@ -585,6 +587,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
       F.j0 = j0; F.k0 = k0; F.nj = j1 - j0 + 1; F.nk = k1 - k0 + 1;
       CK(dalloc(s, &F.trac, (size_t)12 * 9 * (F.nj + 6) * (F.nk + 6)), "fault traction scratch");
     }
+    CK(dalloc(s, &F.gather, (size_t)CGFD_FAULT_NFIELD * g.nj * g.nk), "fault output staging");
     s->faults.push_back(F);
   }
   // stations
@@ -1033,14 +1036,14 @@ int cgfd_dt_max(const cgfd_solver *s, float *d) {
 int cgfd_get_fault_all(cgfd_solver *s, int f, float *out) {
   if (!s || !out || f < 0 || f >= (int)s->faults.size()) return fail(CGFD_ERR_ARG, "bad argument");
   const Grid &g = s->g;
-  const size_t ns = (size_t)g.ny * g.nz;
-  for (int q = 0; q < CGFD_FAULT_NFIELD; q++) {
-    const float *src = s->faults[f].out + q * ns + (size_t)NG * g.ny + NG;
-    cudaError_t e = cudaMemcpy2DAsync(out + (size_t)q * g.nk * g.nj, (size_t)g.nj * 4, src, (size_t)g.ny * 4,
-                                      (size_t)g.nj * 4, g.nk, cudaMemcpyDeviceToHost, s->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "read fault");
-  }
-  cudaError_t e = cudaStreamSynchronize(s->stream);
+  // gather the interior nodes on the device, then one contiguous copy
+  launch_fault_gather(s->faults[f].out, s->faults[f].gather, CGFD_FAULT_NFIELD, g, s->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, s->faults[f].gather, (size_t)CGFD_FAULT_NFIELD * g.nj * g.nk * 4,
+                        cudaMemcpyDeviceToHost, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "read fault");
+  e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read fault");
   return CGFD_OK;
 }

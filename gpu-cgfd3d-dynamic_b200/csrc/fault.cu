@@ -757,4 +757,24 @@ void launch_record(const StationArgs &a, cudaStream_t st) {
 
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(c, max_rec); }
 
+namespace {
+// the interior nodes of the fault output fields [nf][ny*nz] into a
+// contiguous [nf][nk][nj] array, so that one copy brings them to the host
+__global__ void k_fault_gather(const float *__restrict__ out, float *__restrict__ dst, int nf, int nj, int nk,
+                               int ny, long ns) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n = (long)nj * nk;
+  if (t >= n * nf) return;
+  const int q = (int)(t / n);
+  const long r = t - q * n;
+  const int k = (int)(r / nj), j = (int)(r - (long)k * nj);
+  dst[t] = __ldg(out + q * ns + (j + NG) + (long)(k + NG) * ny);
+}
+}  // namespace
+
+void launch_fault_gather(const float *out, float *dst, int nf, const Grid &g, cudaStream_t st) {
+  const long n = (long)nf * g.nj * g.nk;
+  k_fault_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, dst, nf, g.nj, g.nk, g.ny, (long)g.ny * g.nz);
+}
+
 }  // namespace cgfd
