@@ -117,8 +117,6 @@ struct cgfd_solver {
   long long launches_per_step = 0, last_launches = 0;
   int ychunk = 16;                      // interior kernel: y tiles per z-marching chunk (set at upload)
   bool pack = true;                     // pack boxes at most 24 points wide (x PML slabs)
-  int box_top[1][6];                    // rows under the free surface
-  int box_in[1][6];                     // interior box (no PML, no surface rows)
   // boxes of each volume kernel kind: 0 interior, 1 generic shell (PML
   // edges / corners, surface rows), 2..4 slabs reached by the PML faces of
   // one direction only (x, y, z)
@@ -611,13 +609,11 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   }
   st.idx = s->sta_idx; st.w = s->sta_w; st.fid = s->fsta_fid; st.fidx = s->fsta_idx; st.fw = s->fsta_w;
   st.seis = s->seis; st.fseis = s->fseis;
-  // interior box and shell boxes (interior indices, inclusive)
+  // boxes of the volume kernel kinds (interior indices, inclusive)
   {
     auto L = [&](int d, int sd) { return H.pml[d][sd].on ? H.pml[d][sd].L + 1 : 0; };
     const int ilo = L(0, 0), ihi = g.ni - 1 - L(0, 1), jlo = L(1, 0), jhi = g.nj - 1 - L(1, 1);
     const int klo = L(2, 0), khi = s->isfree ? g.nk - 5 : g.nk - 1 - L(2, 1);
-    const int bi[6] = { ilo, ihi, jlo, jhi, klo, khi };
-    std::memcpy(s->box_in[0], bi, sizeof bi);
     auto add = [&](int kind, int i0, int i1, int j0, int j1, int k0, int k1) {
       if (i1 < i0 || j1 < j0 || k1 < k0) return;
       int *b = s->kbox[kind][s->nkbox[kind]++];
@@ -650,8 +646,6 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
       add(5, ilo, ihi, 0, jlo - 1, khi + 1, nk - 1);
       add(5, ilo, ihi, jhi + 1, nj - 1, khi + 1, nk - 1);
     }
-    const int bt[6] = { 0, g.ni - 1, 0, g.nj - 1, s->isfree ? g.nk - 4 : g.nk, g.nk - 1 };
-    std::memcpy(s->box_top[0], bt, sizeof bt);
     // a stage's first fault kernels read its input at i0-6..i0+6 over the
     // split box grown by 3 nodes: when that region meets no PML slab or edge
     // box for any fault, they may start before those kernels of the

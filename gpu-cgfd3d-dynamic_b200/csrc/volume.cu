@@ -15,10 +15,13 @@
 // The reference runs these as 9-10 launches per stage plus three full
 // read-modify-write sweeps of the wavefield for the RK update.  Here the
 // domain is cut into boxes: the interior box (no PML, no surface rows) runs
-// k_volume<INTERIOR>, whose code holds no boundary logic, and the shell of
-// PML slabs and the top four rows runs k_volume<SHELL>.  Each stage reads
-// the input level (stencil taps come from L1/L2), the metric and the medium
-// once and writes the output levels once.
+// k_volume<INTERIOR>, whose code holds no boundary logic; slabs that one
+// direction's PML faces reach run k_volume<FACE_X/Y/Z>; PML edges, corners
+// and the bottom ring run k_volume<EDGE>; the four rows under the free
+// surface run k_volume<SHELL>.  Each stage reads the input level (stencil
+// taps come from L1/L2), the metric and the medium once and writes the
+// output levels once; each thread asks L2 early for the lines it reads
+// last (prefetch), and interior threads for the next z row's DRAM misses.
 //
 // A level stores the nine components of a point in two 16-byte groups and
 // one float (Grid::w), so a stencil tap is three loads: x taps are
