@@ -315,6 +315,7 @@ def main():
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s2 = cgfd.Solver(prob, setup=setup)
+    t_up = time.perf_counter() - t0
     for _ in range(ke):
         s2.run(1)
         s2.fault_all(out_ptr=pinned.data_ptr())
@@ -325,7 +326,8 @@ def main():
     up = setup.upload_bytes
     e2e = {"value": prob.points * ke * ws / e2e_s / 1e9, "unit": unit,
            "h2d_bytes_per_step": int(up / ke), "d2h_bytes_per_step": int(nbytes_f + seis.nbytes / ke),
-           "steps": ke, "note": "upload of the prepared problem amortised over the steps; host set-up excluded"}
+           "steps": ke, "upload_s": round(t_up, 4), "steps_s": round(e2e_s - t_up, 4),
+           "note": "upload of the prepared problem amortised over the steps; host set-up excluded"}
 
     line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": run_ms_max / args.steps, "higher_is_better": True,
