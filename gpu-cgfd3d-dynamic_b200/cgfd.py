@@ -215,6 +215,7 @@ def load_library(path: str = LIB_PATH):
     lib.cgfd_get_fault_stations.argtypes = [vp, _fp, _ip]
     lib.cgfd_get_wavefield.argtypes = [vp, C.c_int, _fp]
     lib.cgfd_get_surface_peaks.argtypes = [vp, _fp]
+    lib.cgfd_release_cached_memory.argtypes = []
     lib.cgfd_set_wavefield.argtypes = [vp, C.c_int, _fp]
     lib.cgfd_checkpoint_size.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     lib.cgfd_checkpoint.argtypes = [vp, vp, C.c_ulonglong]

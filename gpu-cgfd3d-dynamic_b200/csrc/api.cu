@@ -138,9 +138,27 @@ struct cgfd_setup {
 
 namespace {
 
+// Solver memory comes from the device's stream-ordered pool, which keeps
+// freed blocks (release threshold at its maximum) so that a solver created
+// after another one was destroyed reuses its memory instead of mapping new
+// pages; cgfd_release_cached_memory hands the cached blocks back.
+cudaError_t keep_pool_memory() {
+  static std::atomic<unsigned long long> done{ 0 };
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev >= 64 || (done.load() & (1ull << dev))) return e;
+  cudaMemPool_t pool;
+  if ((e = cudaDeviceGetDefaultMemPool(&pool, dev)) != cudaSuccess) return e;
+  unsigned long long thr = ~0ull;
+  if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr)) != cudaSuccess) return e;
+  done.fetch_or(1ull << dev);
+  return cudaSuccess;
+}
+
 template <class T>
 cudaError_t dalloc(cgfd_solver *s, T **p, size_t n) {
-  cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+  cudaError_t e = keep_pool_memory();
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), s->stream);
   if (e == cudaSuccess) { s->allocs.push_back(*p); e = cudaMemsetAsync(*p, 0, std::max<size_t>(n, 1) * sizeof(T), s->stream); }
   return e;
 }
@@ -168,8 +186,11 @@ void destroy(cgfd_solver *s) {
     for (int b = 0; b < 3; b++) if (s->ev_join[a][b]) cudaEventDestroy(s->ev_join[a][b]);
   }
   for (int q = 0; q < 3; q++) if (s->aux[q]) cudaStreamDestroy(s->aux[q]);
-  for (void *p : s->allocs) cudaFree(p);
-  if (s->stream) cudaStreamDestroy(s->stream);
+  for (void *p : s->allocs) cudaFreeAsync(p, s->stream);
+  if (s->stream) {
+    cudaStreamSynchronize(s->stream);
+    cudaStreamDestroy(s->stream);
+  }
   delete s;
 }
 
@@ -391,6 +412,16 @@ int cgfd_setup_dt_max(const cgfd_setup *su, float *d) {
   if (!su || !d) return fail(CGFD_ERR_ARG, "bad argument");
   *d = su->H.dtmax;
   return CGFD_OK;
+}
+
+int cgfd_release_cached_memory(void) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  cudaMemPool_t pool;
+  if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&pool, dev);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  return e == cudaSuccess ? CGFD_OK : cuda_fail(e, "release cached memory");
 }
 
 int cgfd_select_device(int ordinal) {

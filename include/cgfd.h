@@ -168,6 +168,13 @@ void cgfd_setup_free(cgfd_setup *su);
  * calls that follow (the reference's gpu_id_start argument of main). */
 int cgfd_select_device(int ordinal);
 
+/* Device memory of solvers comes from the current device's stream-ordered
+ * memory pool, which keeps the blocks of destroyed solvers for the next
+ * ones (no counterpart in the reference, which calls cudaMalloc / cudaFree
+ * around each run).  This returns the cached blocks of the current device
+ * to the system, after waiting for the device to be idle. */
+int cgfd_release_cached_memory(void);
+
 /* Fill cfg with the reference's defaults (welded margin 40, dynamic
  * method 2, stability check on, no PML, free surface off). */
 void cgfd_config_default(cgfd_config *cfg);

@@ -254,3 +254,19 @@ def test_interior_chunk_choice_changes_nothing(cgfd_lib, monkeypatch):
     assert np.array_equal(g1.fault("Vs"), g2.fault("Vs"))
     for c in range(9):
         assert np.array_equal(g1.wavefield(c), g2.wavefield(c)), WAVE_COMPONENTS[c]
+
+
+def test_pool_reuse_and_release(cgfd_lib):
+    """Solver memory comes from the device's memory pool: a solver made after
+    another was destroyed reuses its blocks and runs the same, and the
+    cached blocks can be handed back."""
+    p = inputs.small_planar(nt=6)
+    g = Solver(p)
+    g.run(6)
+    ref = g.wavefield("Vz").copy()
+    g.close()
+    g2 = Solver(p)
+    g2.run(6)
+    assert np.array_equal(g2.wavefield("Vz"), ref)
+    g2.close()
+    assert cgfd_lib.cgfd_release_cached_memory() == 0
