@@ -202,3 +202,31 @@ def test_sponge_masks_one_step(oracle_built):
     assert np.array_equal(inner, np.ones_like(inner))
     # a corner point takes the smallest of its masks
     np.testing.assert_allclose(ratio[0, 0, 0], mask[0], rtol=3e-6)
+
+
+def test_surface_peaks_against_numpy(oracle_built):
+    """The oracle's peak surface motion (PG_calcu_gpu, src/forward/wav_t.cu:138-216)
+    against the same maxima computed in numpy from the surface velocities of
+    every step: peak |V| and components, peak |dV/dt|, and peak |D| of the
+    trapezoid-rule displacement."""
+    from oracle import OracleSolver
+    p = inputs.small_planar(nt=20)
+    o = OracleSolver(p)
+    dt = np.float32(p.dt)
+    prev = np.zeros((3, p.nj, p.ni), np.float32)
+    disp = np.zeros((3, p.nj, p.ni), np.float64)
+    pk = np.zeros((15, p.nj, p.ni), np.float64)
+    for _ in range(20):
+        o.run(1)
+        v = np.stack([o.wavefield(c)[-1] for c in ("Vx", "Vy", "Vz")]).astype(np.float32)
+        a = np.abs((v - prev) / dt)
+        disp += 0.5 * (v + prev).astype(np.float64) * float(dt)
+        d = disp.astype(np.float32)
+        vals = [np.sqrt((v ** 2).sum(0)), np.sqrt((v[:2] ** 2).sum(0)), *np.abs(v),
+                np.sqrt((a ** 2).sum(0)), np.sqrt((a[:2] ** 2).sum(0)), *a,
+                np.sqrt((d ** 2).sum(0)), np.sqrt((d[:2] ** 2).sum(0)), *np.abs(d)]
+        pk = np.maximum(pk, np.stack(vals))
+        prev = v
+    got = o.surface_peaks()
+    assert got[0].max() > 0
+    np.testing.assert_allclose(got, pk, rtol=2e-5, atol=1e-12 * float(np.abs(pk).max()))
