@@ -167,3 +167,19 @@ def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, case):
         assert not v[:3].any() and not v[:, :3].any()
     assert mine[0].max() > 0
     assert list(np.ravel(pg["_attrs"]["count_index_of_physical_points"])) == [p.ni, p.nj]
+
+
+def test_case_writer_boundary_blocks(tmp_path):
+    """par.json of a sponge case: "ablexp" {number_of_layers, ref_vel} on the
+    five absorbing faces and "free" on the top, as par_t.cu:160-312 reads them."""
+    p = dataclasses.replace(inputs.small_planar(nt=4, pml=0), ablexp_layers=((6, 6), (5, 5), (4, 0)),
+                            ablexp_ref_vel=((6000.0, 5900.0), (5800.0, 5700.0), (5600.0, 5500.0)))
+    par = json.load(open(par_files.write_case(p, str(tmp_path / "case"), nt=4)))
+    names = [("boundary_x_left", 0, 0), ("boundary_x_right", 0, 1), ("boundary_y_front", 1, 0),
+             ("boundary_y_back", 1, 1), ("boundary_z_bottom", 2, 0)]
+    for key, d, s in names:
+        blk = par[key]["ablexp"]
+        assert blk["number_of_layers"] == p.ablexp_layers[d][s]
+        assert blk["ref_vel"] == p.ablexp_ref_vel[d][s]
+        assert "cfspml" not in par[key]
+    assert "free" in par["boundary_z_top"]
