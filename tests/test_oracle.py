@@ -230,3 +230,19 @@ def test_surface_peaks_against_numpy(oracle_built):
     got = o.surface_peaks()
     assert got[0].max() > 0
     np.testing.assert_allclose(got, pk, rtol=2e-5, atol=1e-12 * float(np.abs(pk).max()))
+
+
+def test_sponge_rupture_float_vs_double(oracle_built):
+    """A rupture with the sponge boundary: the float32 oracle (the reference's
+    arithmetic) against the float64 build, slip rate, slip and surface peaks."""
+    import dataclasses
+    from oracle import OracleSolver
+    p = dataclasses.replace(inputs.small_planar(nt=40, pml=0), ablexp_layers=((6, 6), (6, 6), (6, 0)),
+                            ablexp_ref_vel=((6000.0, 6000.0),) * 3)
+    o32, o64 = OracleSolver(p), OracleSolver(p, double=True)
+    o32.run(40)
+    o64.run(40)
+    assert o64.fault("Vs").max() > 0.1
+    for f in ("Vs", "Slip", "Ts1"):
+        assert _rel(o32.fault(f), o64.fault(f)) < 1e-4, f
+    assert _rel(o32.surface_peaks(), o64.surface_peaks()) < 1e-4
