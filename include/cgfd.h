@@ -149,7 +149,9 @@ int cgfd_abi_version(void);
 
 /* Host half of cgfd_create: grid, metric, medium, PML, free-surface and
  * fault set-up into host memory (main_curv_col_el_3d.cu:113-705).  Needs
- * no GPU. */
+ * no GPU; when a device is present, the packed metric and medium are kept
+ * in page-locked host memory so that cgfd_upload copies them at link rate
+ * (this initialises the CUDA context of the current device). */
 int cgfd_prepare(const cgfd_config *cfg, cgfd_setup **out);
 /* Bytes that cgfd_upload copies to the device. */
 int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes);
