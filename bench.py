@@ -11,7 +11,8 @@ A step is one full time step (4 RK stages) of the whole domain.
 
 Prints one JSON line (rank 0).  value = grid-point updates per second over
 the K timed steps (CUDA events on the solver's stream, max over ranks);
-inputs (6.6 GB of wavefield levels per GPU) exceed the 126 MB L2, so no
+inputs (four wavefield levels of 9 components: 6.6 GB per GPU on the
+600x300x240 case, 42 GB on 1200x600x400) exceed the 126 MB L2, so no
 flush is needed between steps.  --gpus N runs N independent replicas (one
 per GPU): the forward path does not shard.
 """
@@ -251,7 +252,8 @@ def main():
     metric, unit = "Gpt-updates/s", "Gpt/s"
     config = {"workload": desc, "grid": [prob.nj, prob.ni, prob.nk], "points": prob.points,
               "dt": prob.dt, "dynamic_method": prob.dynamic_method,
-              "l2": "inputs larger than L2 (6.6 GB of wavefield levels), no flush",
+              "l2": f"inputs larger than L2 ({4 * 9 * 4 * (prob.ni + 6) * (prob.nj + 6) * (prob.nk + 6) / 1e9:.1f} GB "
+                    "of wavefield levels), no flush",
               "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
 
     if args.impl == "reference":

@@ -2,6 +2,7 @@
 // file, on one B200.
 //
 //     cgfd_run par.json [gpu_id]
+//     cgfd_run --check par.json     (inputs and host set-up only, no GPU)
 //
 // Replaces `main par.json gpu_id_start` (src/forward/main_curv_col_el_3d.cu)
 // for one GPU: the same par keys (src/forward/par_t.cu:64-720), the same
@@ -19,7 +20,8 @@
 //                               (io_funcs.cu:1827-1880)
 // The time stepping runs in libcgfd (include/cgfd.h).  Par keys of outputs
 // outside the forward path (receiver_line, slice, snapshot, grid / metric /
-// media export) are reported and ignored.
+// media export), keys without effect on one GPU and keys the reference does
+// not read either are reported on stderr and ignored.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -104,8 +106,61 @@ std::vector<float> read_volume(const cgfd_nc::Reader &r, const std::string &name
 
 }  // namespace
 
+// How the driver treats each top-level key of the reference's par file
+// (par_t.cu:64-900 reads them with cJSON, which ignores any other key).
+enum KeyUse { KEY_USED, KEY_NO_OUTPUT, KEY_NO_EFFECT };
+const struct { const char *key; KeyUse use; } kParKeys[] = {
+  { "number_of_total_grid_points_x", KEY_USED }, { "number_of_total_grid_points_y", KEY_USED },
+  { "number_of_total_grid_points_z", KEY_USED }, { "size_of_time_step", KEY_USED },
+  { "number_of_time_steps", KEY_USED }, { "time_window_length", KEY_USED }, { "time_start", KEY_USED },
+  { "time_check_stability", KEY_USED }, { "io_time_skip", KEY_USED }, { "dynamic_method", KEY_USED },
+  { "fault_x_index", KEY_USED }, { "fault_grid", KEY_USED }, { "boundary_x_left", KEY_USED },
+  { "boundary_x_right", KEY_USED }, { "boundary_y_front", KEY_USED }, { "boundary_y_back", KEY_USED },
+  { "boundary_z_bottom", KEY_USED }, { "boundary_z_top", KEY_USED }, { "grid_generation_method", KEY_USED },
+  { "metric_calculation_method", KEY_USED }, { "medium", KEY_USED }, { "output_dir", KEY_USED },
+  { "in_station_file", KEY_USED }, { "fault_station_file", KEY_USED }, { "welded_margin", KEY_USED },
+  // outputs outside the forward path's fault and station files
+  { "receiver_line", KEY_NO_OUTPUT }, { "slice", KEY_NO_OUTPUT }, { "snapshot", KEY_NO_OUTPUT },
+  { "is_export_grid", KEY_NO_OUTPUT }, { "grid_export_dir", KEY_NO_OUTPUT }, { "is_export_metric", KEY_NO_OUTPUT },
+  { "is_export_media", KEY_NO_OUTPUT }, { "media_export_dir", KEY_NO_OUTPUT }, { "output_all", KEY_NO_OUTPUT },
+  // no effect with the whole domain on one GPU, or only a message in the reference
+  { "number_of_mpiprocs_x", KEY_NO_EFFECT }, { "number_of_mpiprocs_y", KEY_NO_EFFECT },
+  { "number_of_mpiprocs_z", KEY_NO_EFFECT }, { "check_nan_every_number_of_steps", KEY_NO_EFFECT },
+  { "visco_config", KEY_NO_EFFECT },
+};
+
+// one line per top-level key that does not change the run: outputs this
+// driver does not write, keys without effect on one GPU, and keys the
+// reference does not read either (cJSON skips them: a leading '#' is the
+// examples' way of commenting a key out; misspelt keys fall here too)
+void report_keys(const Value &par) {
+  for (const auto &kv : par.obj) {
+    const std::string &k = kv.first;
+    int use = -1;
+    for (const auto &e : kParKeys) if (k == e.key) use = e.use;
+    if (use == KEY_USED) continue;
+    if (use == KEY_NO_OUTPUT)
+      std::fprintf(stderr, "cgfd_run: %s: output not produced by this driver, ignored\n", k.c_str());
+    else if (use == KEY_NO_EFFECT)
+      std::fprintf(stderr, "cgfd_run: %s: no effect on a single-GPU run, ignored\n", k.c_str());
+    else if (!k.empty() && k[0] == '#')
+      std::fprintf(stderr, "cgfd_run: %s: commented out, ignored\n", k.c_str());
+    else
+      std::fprintf(stderr, "cgfd_run: %s: not a key of the reference's par file, ignored\n", k.c_str());
+  }
+}
+
 int main(int argc, char **argv) {
-  if (argc < 2) die("usage: cgfd_run par.json [gpu_id]");
+  // --check: parse the par file, read every input file and run the host
+  // set-up (grid, metric, medium, PML, fault coefficients), then report the
+  // configuration and exit; needs no GPU
+  bool check_only = false;
+  if (argc > 1 && std::strcmp(argv[1], "--check") == 0) {
+    check_only = true;
+    argv++;
+    argc--;
+  }
+  if (argc < 2) die("usage: cgfd_run [--check] par.json [gpu_id]");
   const int gpu = argc > 2 ? std::atoi(argv[2]) : 0;
   Value par;
   try {
@@ -113,6 +168,8 @@ int main(int argc, char **argv) {
   } catch (const std::exception &e) {
     die(e.what());
   }
+  if (par.kind != Value::Object) die("par file: a JSON object expected");
+  report_keys(par);
 
   // ---- grid, time ---------------------------------------------------------
   cgfd_config cfg;
@@ -132,6 +189,9 @@ int main(int argc, char **argv) {
     if (twin < 0.0) die("number_of_time_steps or time_window_length needed");
     nt = (int)(twin / dt + 0.5);
   }
+  // the reference's time loop takes number_of_time_steps + 1 steps
+  // (nt_total, main_curv_col_el_3d.cu:483; drv_rk_curv_col.cu:209)
+  const int nt_total = nt + 1;
   const double t0 = num(par, "time_start", 0.0);
   const int skip = std::max(1, (int)num(par, "io_time_skip", 1));
   cfg.dt = (float)dt;
@@ -303,13 +363,24 @@ int main(int argc, char **argv) {
   cfg.num_fault_stations = (int)fsta.size();
   cfg.fault_station_fault = ffault.empty() ? nullptr : ffault.data();
   cfg.fault_station_jk = fjk.empty() ? nullptr : fjk.data();
-  cfg.max_records = nt;
+  cfg.max_records = nt_total;
 
-  for (const char *k : { "receiver_line", "slice", "snapshot", "visco_config" })
-    if (par.get(k)) std::fprintf(stderr, "cgfd_run: %s is not produced by this driver, ignored\n", k);
+  if (const Value *mm = par.get("metric_calculation_method"))
+    if (mm->get("import")) die("metric_calculation_method: import is not supported (the metric is calculated)");
   const std::string out_dir = str(par, "output_dir", ".");
 
   // ---- set-up and run -----------------------------------------------------
+  if (check_only) {
+    cgfd_setup *su = nullptr;
+    check(cgfd_prepare(&cfg, &su), "set-up");
+    float dtmax = 0.f;
+    check(cgfd_setup_dt_max(su, &dtmax), "set-up");
+    cgfd_setup_free(su);
+    std::fprintf(stdout, "grid %d x %d x %d, dt %g (max %g), %d steps, %d fault(s), dynamic_method %d, "
+                 "free surface %d, %d station(s), %d fault station(s)\n", ni, nj, nk, dt, dtmax, nt_total,
+                 cfg.num_faults, cfg.dynamic_method, cfg.free_surface, cfg.num_stations, cfg.num_fault_stations);
+    return 0;
+  }
   check(cgfd_select_device(gpu), "select GPU");
   cgfd_setup *su = nullptr;
   check(cgfd_prepare(&cfg, &su), "set-up");
@@ -349,7 +420,7 @@ int main(int argc, char **argv) {
   std::vector<float> fout((size_t)CGFD_FAULT_NFIELD * nk * nj);
   int it = 0;
   std::fprintf(stdout, "start time loop ...\n");
-  while (it < nt) {
+  while (it < nt_total) {
     if (it % skip == 0) {
       const float tcur = (float)(it * dt + t0);
       for (int f = 0; f < cfg.num_faults; f++) {
@@ -358,7 +429,7 @@ int main(int argc, char **argv) {
         for (int q = 0; q < 9; q++) ff[f].w->put_record_float(ff[f].vf[q], it / skip, fout.data() + (size_t)q * nk * nj);
       }
     }
-    const int n = std::min(skip - it % skip, nt - it);   // up to the next output step
+    const int n = std::min(skip - it % skip, nt_total - it);   // up to the next output step
     check(cgfd_run(s, n), "time step");
     it += n;
   }
@@ -462,6 +533,6 @@ int main(int argc, char **argv) {
     }
   }
   cgfd_destroy(s);
-  std::fprintf(stdout, "done: %d steps\n", nt);
+  std::fprintf(stdout, "done: %d steps\n", nt_total);
   return 0;
 }

@@ -119,15 +119,20 @@ def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, case):
     assert r.returncode == 0, r.stderr
     out = json.load(open(par))["output_dir"]
     ds = [par_files.read_fault_output(os.path.join(out, f"fault_i{x}_px0_py0_pz0.nc")) for x in p.fault_x_index]
+    # the reference's loop takes nt + 1 steps and writes a record before
+    # every io_time_skip-th of them (drv_rk_curv_col.cu:209-227)
+    nt_total = nt + 1
+    nrec = (nt_total + skip - 1) // skip
     for d in ds:
-        assert d["Tn"].shape == (nt // skip, p.nk, p.nj)
+        assert d["Tn"].shape == (nrec, p.nk, p.nj)
+    p.max_records = nt_total
     s = Solver(p)
-    for rec in range(nt // skip):
+    for rec in range(nrec):
         for fi, d in enumerate(ds):
             np.testing.assert_allclose(d["time"][rec], rec * skip * p.dt, rtol=1e-6)
             for q, f in enumerate(par_files.FAULT_CMP):
                 assert np.array_equal(d[f][rec], s.fault(f, fi)), (rec, fi, f)
-        s.run(skip)
+        s.run(min(skip, nt_total - rec * skip))
     for fi, d in enumerate(ds):
         assert np.array_equal(d["Peak_vs"], s.fault("Peak_vs", fi))
         assert np.array_equal(d["Init_t0"], s.fault("Init_t0", fi))
@@ -137,7 +142,7 @@ def test_driver_run_matches_library(cgfd_lib, tmp_path, medium, case):
     for q in range(len(p.stations)):
         for c, name in enumerate(par_files.CMP):
             fh, ih, kh, tr = par_files.read_sac(os.path.join(out, f"s{q}.{name}.sac"))
-            assert ih[9] == nt and np.array_equal(tr, seis[q, c]), (q, name)
+            assert ih[9] == nt_total and np.array_equal(tr, seis[q, c]), (q, name)
         # strain from the stress traces (the reference's conversion)
         i, j, k = [int(v) for v in p.stations[q]]
         lam, mu = float(p.lam[k, j, i]), float(p.mu[k, j, i])
@@ -183,3 +188,119 @@ def test_case_writer_boundary_blocks(tmp_path):
         assert blk["ref_vel"] == p.ablexp_ref_vel[d][s]
         assert "cfspml" not in par[key]
     assert "free" in par["boundary_z_top"]
+
+
+def _template_par_text(case_dir, out_dir, p):
+    """A par file laid out like the reference's shipped template
+    (example/tpv/dynamic-cfspml.sh:53-205): its key set, its '#'-commented
+    keys (some given twice, as the template does), its misspelt
+    "check_nan_every_nummber_of_steps", the "check_stability" key that the
+    reference's reader does not know, and export / line / slice / snapshot
+    blocks; values for the small planar case.  Written as text because JSON
+    objects with repeated keys have no Python dict form."""
+    pml = ('{ "cfspml" : { "number_of_layers" : %d, "alpha_max" : 3.14, "beta_max" : 2.0, '
+           '"ref_vel" : 6000.0 } }' % p.pml_layers[0][0])
+    g = p.fault_grid[0]
+    return f"""{{
+  "number_of_total_grid_points_x" : {p.ni},
+  "number_of_total_grid_points_y" : {p.nj},
+  "number_of_total_grid_points_z" : {p.nk},
+  "number_of_mpiprocs_y" : 1,
+  "number_of_mpiprocs_z" : 1,
+  "size_of_time_step" : {p.dt},
+  "number_of_time_steps" : 4,
+  "#time_window_length" : 10,
+  "check_stability" : 1,
+  "io_time_skip" : 1,
+  "dynamic_method" : {p.dynamic_method},
+  "fault_grid" : [{g[0]}, {g[1]}, {g[2]}, {g[3]}],
+  "fault_x_index" : [ {p.fault_x_index[0]} ],
+  "welded_margin" : {p.welded_margin},
+  "grid_generation_method" : {{
+      "fault_plane" : {{
+        "fault_geometry_dir" : "{case_dir}/fault_coord",
+        "fault_init_stress_dir" : "{case_dir}/init_stress",
+        "fault_inteval" : {p.fault_interval}
+      }},
+      "#grid_import" : {{ "import_dir" : "{case_dir}", "fault_init_stress_dir" : "{case_dir}" }}
+  }},
+  "is_export_grid" : 1,
+  "grid_export_dir"   : "{out_dir}",
+  "boundary_x_left" : {pml},
+  "boundary_x_right" : {pml},
+  "boundary_y_front" : {pml},
+  "boundary_y_back" : {pml},
+  "boundary_z_bottom" : {pml},
+  "boundary_z_top" : {{ "free" : "timg" }},
+  "metric_calculation_method" : {{ "#import" : "{out_dir}", "calculate" : 1 }},
+  "is_export_metric" : 1,
+  "medium" : {{
+      "type" : "elastic_iso",
+      "#input_way" : "infile_layer",
+      "#input_way" : "binfile",
+      "input_way" : "code",
+      "#binfile" : {{ "size" : [11, 14, 12], "spacing" : [-10, 10, 10], "origin" : [0.0, 0.0, 0.0],
+                     "dim1" : "z", "dim2" : "x", "dim3" : "y" }},
+      "#import" : "{out_dir}",
+      "code" : "",
+      "#equivalent_medium_method" : "loc",
+      "#equivalent_medium_method" : "har"
+  }},
+  "is_export_media" : 1,
+  "media_export_dir"  : "{out_dir}",
+  "#visco_config" : {{ "type" : "graves_Qs", "Qs_freq" : 1.0 }},
+  "output_dir" : "{out_dir}",
+  "in_station_file" : "{case_dir}/stations.txt",
+  "fault_station_file" : "{case_dir}/fault_stations.txt",
+  "#receiver_line" : [ {{ "name" : "line_x_1", "grid_index_start" : [ 1, 9, 9 ],
+                         "grid_index_incre" : [ 1, 0, 0 ], "grid_index_count" : 5 }} ],
+  "#slice" : {{ "x_index" : [ 11 ], "y_index" : [ 12 ], "z_index" : [ 13 ] }},
+  "#snapshot" : [ {{ "name" : "volume_vel", "grid_index_start" : [ 1, 1, {p.nk} ],
+                    "grid_index_count" : [ {p.ni}, {p.nj}, 1 ], "grid_index_incre" : [ 1, 1, 1 ],
+                    "time_index_start" : 0, "time_index_incre" : 1, "save_velocity" : 1,
+                    "save_stress" : 0, "save_strain" : 0 }} ],
+  "check_nan_every_nummber_of_steps" : 0,
+  "output_all" : 0
+}}
+"""
+
+
+def test_driver_accepts_the_reference_par_template(cgfd_lib, tmp_path):
+    """cgfd_run --check (inputs and host set-up, no GPU) on a par file laid
+    out like the reference's own template: every key is either used or
+    reported as ignored, and the run is configured as the reference would
+    configure it (the uniform medium of input_way "code", 4 + 1 steps)."""
+    from cgfd import Problem  # noqa: F401
+    lam, mu, rho = inputs._homog(36, 56, 32)
+    p = inputs.small_planar(nt=4)
+    p.lam, p.mu, p.rho = lam, mu, rho
+    case = str(tmp_path / "case")
+    par_files.write_case(p, case, nt=4, medium="code")
+    fs = os.path.join(case, "fault_stations.txt")
+    if not os.path.exists(fs):
+        with open(fs, "w") as fh:
+            fh.write("1\nf0 1 28.0 22.0\n")
+    out = str(tmp_path / "out")
+    os.makedirs(out)
+    par = tmp_path / "template.json"
+    par.write_text(_template_par_text(case, out, p))
+    exe = os.path.join(ROOT, "gpu-cgfd3d-dynamic_b200", "lib", "cgfd_run")
+    r = subprocess.run([exe, "--check", str(par)], capture_output=True, text=True, timeout=120,
+                       env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+    assert r.returncode == 0, r.stderr
+    err = r.stderr
+    for k in ("#time_window_length", "#visco_config", "#receiver_line", "#slice", "#snapshot"):
+        assert f"{k}: commented out, ignored" in err, k
+    for k in ("check_stability", "check_nan_every_nummber_of_steps"):
+        assert f"{k}: not a key of the reference's par file, ignored" in err, k
+    for k in ("is_export_grid", "grid_export_dir", "is_export_metric", "is_export_media", "media_export_dir",
+              "output_all"):
+        assert f"{k}: output not produced by this driver, ignored" in err, k
+    for k in ("number_of_mpiprocs_y", "number_of_mpiprocs_z"):
+        assert f"{k}: no effect on a single-GPU run, ignored" in err, k
+    for k in ("number_of_total_grid_points_x", "medium", "metric_calculation_method", "boundary_z_top"):
+        assert f"{k}:" not in err, k
+    want = (f"grid {p.ni} x {p.nj} x {p.nk}, dt {p.dt:g}", "5 steps", "1 fault(s), dynamic_method 2",
+            "free surface 1", f"{len(p.stations)} station(s)")
+    for w in want:
+        assert w in r.stdout, (w, r.stdout)
