@@ -198,49 +198,67 @@ def oracle_rate(prob, steps, warmup, budget_s=150.0):
 def ensemble_main(args):
     """Scenarios per hour of 1500-step runs, from --steps timed steps of
     every scenario: the ensemble (one graph launch per step, a branch per
-    scenario) against looping cgfd_run over the same solvers."""
+    scenario) against looping cgfd_run over the same solvers.  Under
+    torchrun the scenarios are partitioned across the ranks by cost (points
+    x steps, shard.partition), each rank running its share as one ensemble
+    on its own GPU; the job's time is the slowest rank's."""
     import torch
     import cgfd
     import inputs
-    torch.cuda.set_device(0)
+    import shard
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
     probs = inputs.ensemble_scenarios(args.ensemble, nt=args.warmup + 2 * args.steps + 16)
-    solvers = [cgfd.Solver(p) for p in probs]
+    parts = shard.partition([shard.scenario_cost(p, 1500) for p in probs], ws)
+    mine = [probs[q] for q in parts[rank]]
+    solvers = [cgfd.Solver(p) for p in mine]
     pts = sum(p.points for p in probs)
     for s in solvers:                              # warm-up: graphs of every operator pair
         s.run(max(args.warmup, 8))
     torch.cuda.synchronize()
+    barrier(ws)
     t0 = time.perf_counter()
     for s in solvers:
         s.run(args.steps)
     torch.cuda.synchronize()
-    t_loop = time.perf_counter() - t0
-    ens = cgfd.Ensemble(solvers)
-    ens.run(8)
+    t_loop = allmax(ws, time.perf_counter() - t0)
+    ens = cgfd.Ensemble(solvers) if solvers else None
+    if ens:
+        ens.run(8)
     torch.cuda.synchronize()
-    clk = ClockSampler(0)
+    clk = ClockSampler(local)
     clk.wait_first_sample()
+    barrier(ws)
     t_start = time.time()
     t0 = time.perf_counter()
-    ens.run(args.steps)
+    if ens:
+        ens.run(args.steps)
     torch.cuda.synchronize()
-    t_ens = time.perf_counter() - t0
+    t_ens = allmax(ws, time.perf_counter() - t0)
     clocks = clk.stop(t_start, time.time())
     full = 1500
     rate = lambda t: len(probs) * 3600.0 / (t * full / args.steps)
     line = {"metric": "ensemble scenarios/hour", "value": rate(t_ens), "unit": "scenarios/h",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "strong",
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{len(probs)} seeded scenarios (inputs.ensemble_scenarios): grids "
                                    "64-160 x 96-256 x 64-128, h 100-200 m, von Karman shear stress, random "
                                    "nucleation, mu_s 0.6-0.7, Dc 0.2-0.5 m, half with hill topography; "
                                    f"{full}-step runs, rate from {args.steps} timed steps of every scenario",
-                       "points": pts},
+                       "points": pts,
+                       "parallelism": f"scenarios partitioned by cost over {ws} GPUs" if ws > 1 else "single GPU"},
             "loop": {"value": rate(t_loop), "unit": "scenarios/h",
                      "note": "cgfd_run over the same solvers one after another"},
             "speedup_vs_loop": t_loop / t_ens,
             "gpt_per_s": pts * args.steps / t_ens / 1e9, "clocks": clocks}
-    ens.close()
-    print(json.dumps(line), flush=True)
+    if ens:
+        ens.close()
+    barrier(ws)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    import replicas
+    replicas.finish(ws)
 
 
 def main():
