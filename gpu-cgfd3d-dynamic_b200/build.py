@@ -1,4 +1,5 @@
-"""Build libcgfd.so (sm_100a) in-tree: gpu-cgfd3d-dynamic_b200/lib/libcgfd.so.
+"""Build libcgfd.so (sm_100a) in-tree: gpu-cgfd3d-dynamic_b200/lib/libcgfd.so,
+and libcgfd64.so, the same kernels computing in double.
 
 nvcc cross-compiles for sm_100a without a GPU; the host set-up is g++ with
 OpenMP.  Objects go to gpu-cgfd3d-dynamic_b200/_build/.
@@ -13,18 +14,21 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcgfd.so")
+# the same kernels computing in double (-DCGFD_FP64), for error statements
+# of the float build against a double build on the same inputs
+LIB64 = os.path.join(LIBDIR, "libcgfd64.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 
 # (source, object, extra flags): the volume kernels build as one unit per
 # kernel kind so that they compile in parallel
-CU = [("volume.cu", f"volume_k{k}.cu.o", [f"-DCGFD_VOLUME_KIND={k}"]) for k in range(6)] + [
+CU = [("volume.cu", f"volume_k{k}.cu.o", [f"-DCGFD_VOLUME_KIND={k}"]) for k in range(7)] + [
     (f, f + ".o", []) for f in ("fault.cu", "boundary.cu", "noalloc.cu", "api.cu")]
 CPP = ["setup.cpp"]
 DRIVER = os.path.join(HERE, "driver")
 DRIVER_SRC = ["cgfd_run.cpp", "ncclassic.cpp", "sac.cpp"]
 DRIVER_BIN = os.path.join(HERE, "lib", "cgfd_run")
-HEADERS = ["common.h", "ops.cuh", "setup.h"]
+HEADERS = ["common.h", "ops.cuh", "setup.h", "real.h"]
 
 
 def _newer(dst, srcs):
@@ -48,15 +52,17 @@ def build(verbose=False, ptxas_info=False):
             subprocess.check_call(cmd)
         objs.append(obj)
     jobs = []
-    for f, o, extra in CU:
-        src, obj = os.path.join(CSRC, f), os.path.join(BUILD, o)
-        if _newer(obj, [src] + hdrs) or ptxas_info:
-            cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                                   "--expt-relaxed-constexpr"] + extra + ["-c", src, "-o", obj]
-            if ptxas_info:
-                cmd += ["-Xptxas", "-v"]
-            jobs.append(cmd)
-        objs.append(obj)
+    objs64 = list(objs)
+    for variant, defs, dst in (("", [], objs), ("64", ["-DCGFD_FP64"], objs64)):
+        for f, o, extra in CU:
+            src, obj = os.path.join(CSRC, f), os.path.join(BUILD, o.replace(".o", variant + ".o"))
+            if _newer(obj, [src] + hdrs) or (ptxas_info and not variant):
+                cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                                       "--expt-relaxed-constexpr"] + defs + extra + ["-c", src, "-o", obj]
+                if ptxas_info and not variant:
+                    cmd += ["-Xptxas", "-v"]
+                jobs.append(cmd)
+            dst.append(obj)
     if jobs:
         from concurrent.futures import ThreadPoolExecutor
         if verbose:
@@ -69,11 +75,12 @@ def build(verbose=False, ptxas_info=False):
                 sys.stderr.write(r.stdout + r.stderr)
             if r.returncode != 0:
                 raise subprocess.CalledProcessError(r.returncode, cmd)
-    if _newer(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp"]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
+    for lib, ob in ((LIB, objs), (LIB64, objs64)):
+        if _newer(lib, ob):
+            cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + ob + ["-lgomp"]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.check_call(cmd)
     # the par-file driver, linked against the library with an rpath to it
     dsrc = [os.path.join(DRIVER, f) for f in DRIVER_SRC]
     dhdr = [os.path.join(DRIVER, f) for f in ("json.h", "ncclassic.h", "sac.h")] + hdrs

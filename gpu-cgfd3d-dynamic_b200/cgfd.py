@@ -20,6 +20,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("CGFD_LIB", os.path.join(HERE, "lib", "libcgfd.so"))
+# the same kernels computing in double, for error statements of the float build
+LIB64_PATH = os.path.join(HERE, "lib", "libcgfd64.so")
 
 MAX_FAULTS = 8
 GRID_FAULT_PLANE = 0
@@ -191,14 +193,14 @@ class CgfdError(RuntimeError):
     pass
 
 
-_lib = None
+_libs = {}
 
 
 def load_library(path: str = LIB_PATH):
-    """Load libcgfd.so; raises if it has not been built."""
-    global _lib
-    if _lib is not None:
-        return _lib
+    """Load libcgfd.so (or, given its path, libcgfd64.so); raises if it has
+    not been built."""
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
         raise CgfdError(f"libcgfd.so not built at {path}: run build.py (or __graft_entry__.build())")
     lib = C.CDLL(path)
@@ -233,14 +235,21 @@ def load_library(path: str = LIB_PATH):
     lib.cgfd_set_timing.argtypes = [vp, C.c_int]
     lib.cgfd_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     lib.cgfd_run_noalloc.argtypes = [vp, C.c_int]
+    lib.cgfd_run_fault_output.argtypes = [vp, C.c_int, C.c_int, vp, C.c_longlong, _ip]
     lib.cgfd_ensemble_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
     lib.cgfd_ensemble_run.argtypes = [vp, C.c_int]
     lib.cgfd_ensemble_destroy.argtypes = [vp]
     lib.cgfd_ensemble_destroy.restype = None
     lib.cgfd_last_kernel_timing.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                             C.POINTER(C.c_longlong)]
-    _lib = lib
+    _libs[path] = lib
     return lib
+
+
+def load_library64():
+    """libcgfd64.so: the solver's kernels built to compute and store in
+    double, behind the same C ABI (float inputs widened, outputs narrowed)."""
+    return load_library(LIB64_PATH)
 
 
 def _fptr(a):
@@ -326,6 +335,26 @@ class Solver:
 
     def run(self, nsteps: int):
         self._check(self.lib.cgfd_run(self.h, int(nsteps)))
+
+    def run_fault_output(self, nsteps: int, every: int = 1, out_ptr: int = None, max_records: int = None):
+        """Advance nsteps steps, taking the fault fields before every step
+        whose index is a multiple of `every` (cgfd_run_fault_output).  With
+        out_ptr (e.g. a page-locked buffer's address) the records go there
+        and their count is returned; otherwise a new array
+        [records, faults, 11, nk, nj] is returned."""
+        p = self.prob
+        start = self.steps_done
+        want = sum(1 for q in range(nsteps) if (start + q) % every == 0)
+        n = C.c_int()
+        if out_ptr is not None:
+            cap = want if max_records is None else max_records
+            self._check(self.lib.cgfd_run_fault_output(self.h, int(nsteps), int(every), C.c_void_p(out_ptr),
+                                                       int(cap), C.byref(n)))
+            return n.value
+        out = np.empty((max(want, 1), p.num_faults, 11, p.nk, p.nj), np.float32)
+        self._check(self.lib.cgfd_run_fault_output(self.h, int(nsteps), int(every), out.ctypes.data_as(C.c_void_p),
+                                                   int(want), C.byref(n)))
+        return out[:n.value]
 
     @property
     def steps_done(self):

@@ -32,12 +32,13 @@ void launch_volume_face_x(const VolArgs &a, int idir, int jdir, int kdir, int mo
 void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_edge(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume_plane(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 int launch_fault_pre(const FaultArgs &a, cudaStream_t st);
 int launch_fault_post(const FaultArgs &a, cudaStream_t st);
-cudaError_t noalloc_scratch_address(float **p);
+cudaError_t noalloc_scratch_address(real **p);
 void launch_record(const StationArgs &a, cudaStream_t st);
 void launch_advance(Ctl *c, int max_rec, cudaStream_t st);
-void launch_fault_gather(const float *out, float *dst, int nf, const Grid &g, cudaStream_t st);
+void launch_fault_gather(const real *out, real *dst, int nf, const Grid &g, cudaStream_t st);
 int launch_sponge(const SpongeArgs &a, cudaStream_t st);
 int launch_surface_peaks(const PeakArgs &a, cudaStream_t st);
 }  // namespace cgfd
@@ -54,23 +55,23 @@ int fail(int code, const std::string &m) { g_err = m; g_err_is_fixed = false; re
 
 // FD_Flags (src/forward/fd_t.cu:146-159): 0 backward, 1 forward
 const int kPairs[8][3] = { {0,0,0},{1,1,0},{1,1,1},{0,0,1},{0,1,0},{1,0,0},{1,0,1},{0,1,1} };
-const float kRkA[3] = { 0.5f, 0.5f, 1.0f };
-const float kRkB[4] = { 1.0f / 6.0f, 1.0f / 3.0f, 1.0f / 3.0f, 1.0f / 6.0f };
+const real kRkA[3] = { RL(0.5), RL(0.5), RL(1.0) };
+const real kRkB[4] = { RL(1.0) / RL(6.0), RL(1.0) / RL(3.0), RL(1.0) / RL(3.0), RL(1.0) / RL(6.0) };
 
 struct FaultState {
   FaultDev d;
   int j0 = 0, k0 = 0, nj = 0, nk = 0;   // bounding box of split nodes (interior)
-  float *lev[4] = {};                   // storage slots, [9][2][ny*nz]
+  real *lev[4] = {};                    // storage slots, [9][2][ny*nz]
   uint8_t *flag = nullptr;
-  float *mat = nullptr, *fmat = nullptr, *scal = nullptr, *out = nullptr;
-  float *trac = nullptr;                // traction scratch of the split box
-  float *gather = nullptr;              // output fields at interior nodes, [11][nk][nj]
+  real *mat = nullptr, *fmat = nullptr, *scal = nullptr, *out = nullptr;
+  real *trac = nullptr;                 // traction scratch of the split box
+  real *gather = nullptr;               // output fields at interior nodes, [11][nk][nj]
 };
 
 struct PmlState {
   PmlFaceDev d{};
-  float *coef = nullptr;                // A | B | D
-  float *aux[4] = {};
+  real *coef = nullptr;                 // A | B | D
+  real *aux[4] = {};
 };
 
 }  // namespace
@@ -79,18 +80,18 @@ struct cgfd_solver {
   Grid g{};
   int imethod = 2, isfree = 0;
   float dt = 0.f, dtmax = 0.f;
-  float *w[4] = {};                     // storage slots of the 4 levels
-  float *coef = nullptr, *free_mat = nullptr;   // packed metric and medium (13 scmp floats)
-  float *abl_E = nullptr;               // sponge masks [nx | ny | nz]
+  real *w[4] = {};                      // storage slots of the 4 levels
+  real *coef = nullptr, *free_mat = nullptr;    // packed metric and medium (13 scmp values)
+  real *abl_E = nullptr;                // sponge masks [nx | ny | nz]
   SpongeArgs sponge{};                  // sponge blocks (w set per step)
-  float *pg = nullptr, *dis = nullptr;  // surface peaks [15][nj][ni], displacement [3][nj][ni]
+  real *pg = nullptr, *dis = nullptr;   // surface peaks [15][nj][ni], displacement [3][nj][ni]
   PmlState pml[6];
   std::vector<FaultState> faults;
   StationDev st{};
   long *sta_idx = nullptr;
-  float *sta_w = nullptr, *fsta_w = nullptr;
+  real *sta_w = nullptr, *fsta_w = nullptr;
   int *fsta_fid = nullptr, *fsta_idx = nullptr;
-  float *seis = nullptr, *fseis = nullptr;
+  real *seis = nullptr, *fseis = nullptr;
   Ctl *ctl = nullptr;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph[2][8] = {};     // [timing][it % 8]
@@ -110,6 +111,10 @@ struct cgfd_solver {
   // the next stage's first fault kernels may overlap this stage's PML slab
   // and edge kernels (no fault neighbourhood meets their boxes)
   bool pre_early = false;
+  // the interior kernel defers the fault planes x = i0 to a PLANE launch
+  // and so runs beside the stage's first fault kernels (CGFD_PRE_OVERLAP)
+  bool pre_overlap = false;
+  cudaEvent_t ev_stage[4] = {}, ev_predone[4] = {}, ev_postdone[4] = {};
   double run_ms = 0, vol_ms = 0, int_ms = 0;
   long long vol_launches = 0, int_launches = 0;
   long long int_points = 0, vol_points = 0;   // points one launch updates
@@ -120,9 +125,15 @@ struct cgfd_solver {
   // boxes of each volume kernel kind: 0 interior, 1 generic shell (PML
   // edges / corners, surface rows), 2..4 slabs reached by the PML faces of
   // one direction only (x, y, z)
-  int kbox[6][12][6];
-  int nkbox[6] = {};
+  int kbox[7][12][6];
+  int nkbox[7] = {};
   std::vector<void *> allocs;
+  // cgfd_run_fault_output: two device staging buffers of one record (all
+  // faults' 11 fields at interior nodes), a copy stream and the events that
+  // order gather -> copy -> reuse (made on first use)
+  real *rec_buf[2] = {};
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_gathered[2] = {}, ev_copied[2] = {};
 };
 
 struct cgfd_setup {
@@ -137,6 +148,35 @@ struct cgfd_setup {
 };
 
 namespace {
+
+// host floats (the set-up's arrays) to device values of type real on the
+// solver's stream; the double build widens them on the host first and
+// copies synchronously
+cudaError_t to_device(real *dst, const float *src, size_t n, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+#ifdef CGFD_FP64
+  std::vector<double> wide(src, src + n);
+  cudaError_t e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? cudaMemcpy(dst, wide.data(), n * sizeof(double), cudaMemcpyHostToDevice) : e;
+#else
+  return cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyHostToDevice, st);
+#endif
+}
+
+// device values of type real to host floats, waiting for the copy
+cudaError_t to_host(float *dst, const real *src, size_t n, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+#ifdef CGFD_FP64
+  std::vector<double> wide(n);
+  cudaError_t e = cudaMemcpyAsync(wide.data(), src, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) for (size_t q = 0; q < n; q++) dst[q] = (float)wide[q];
+  return e;
+#else
+  cudaError_t e = cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost, st);
+  return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+#endif
+}
 
 // Solver memory comes from the device's stream-ordered pool, which keeps
 // freed blocks (release threshold at its maximum) so that a solver created
@@ -181,11 +221,19 @@ void destroy(cgfd_solver *s) {
     if (s->ev_int0[a][b]) cudaEventDestroy(s->ev_int0[a][b]);
   }
   for (int a = 0; a < 4; a++) {
+    if (s->ev_stage[a]) cudaEventDestroy(s->ev_stage[a]);
+    if (s->ev_predone[a]) cudaEventDestroy(s->ev_predone[a]);
+    if (s->ev_postdone[a]) cudaEventDestroy(s->ev_postdone[a]);
     if (s->ev_fork[a]) cudaEventDestroy(s->ev_fork[a]);
     if (s->ev_pre[a]) cudaEventDestroy(s->ev_pre[a]);
     for (int b = 0; b < 3; b++) if (s->ev_join[a][b]) cudaEventDestroy(s->ev_join[a][b]);
   }
   for (int q = 0; q < 3; q++) if (s->aux[q]) cudaStreamDestroy(s->aux[q]);
+  for (int q = 0; q < 2; q++) {
+    if (s->ev_gathered[q]) cudaEventDestroy(s->ev_gathered[q]);
+    if (s->ev_copied[q]) cudaEventDestroy(s->ev_copied[q]);
+  }
+  if (s->copy) { cudaStreamSynchronize(s->copy); cudaStreamDestroy(s->copy); }
   for (void *p : s->allocs) cudaFreeAsync(p, s->stream);
   if (s->stream) {
     cudaStreamSynchronize(s->stream);
@@ -194,10 +242,31 @@ void destroy(cgfd_solver *s) {
   delete s;
 }
 
-// enqueue one time step (graph capture or direct launches); trac: traction
-// scratch to use instead of each fault's own (cgfd_run_noalloc); timed:
-// whether the solver's timing events may be recorded
-void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = true) {
+// floats of traction scratch a fault's split box needs (12 planes x 9
+// components over the box grown by 3 nodes); 0 for a fault without split
+// nodes
+size_t trac_floats(const FaultState &F) {
+  return F.nj > 0 && F.nk > 0 ? (size_t)12 * 9 * (F.nj + 6) * (F.nk + 6) : 0;
+}
+
+// start of each fault's slice of a shared traction scratch: the slices lie
+// one after another, each on a 64-float (256-byte) boundary; returns the
+// floats all slices take
+size_t trac_slices(const cgfd_solver *s, size_t *off) {
+  size_t n = 0;
+  for (size_t f = 0; f < s->faults.size(); f++) {
+    off[f] = n;
+    n += (trac_floats(s->faults[f]) + 63) / 64 * 64;
+  }
+  return n;
+}
+
+// enqueue one time step (graph capture or direct launches); trac: one
+// traction scratch to use instead of each fault's own (cgfd_run_noalloc),
+// split into one slice per fault because the first fault kernels of every
+// fault run before the later ones of any fault; timed: whether the
+// solver's timing events may be recorded
+void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = true) {
   const int ip = it % 8;
   const bool tm = s->timing && timed;
   long long nl = 0;
@@ -211,11 +280,14 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     const int mode = stage == 0 ? RK_FIRST : (stage == 3 ? RK_LAST : RK_MID);
     const int Lcur = stage == 0 ? LP : (stage == 2 ? LB : LA);
     const int Lout = stage == 0 ? LA : (stage == 1 ? LB : (stage == 2 ? LA : -1));
-    const float ca = stage < 3 ? kRkA[stage] * s->dt : 0.f, cb = kRkB[stage] * s->dt;
+    const real ca = stage < 3 ? kRkA[stage] * s->dt : RL(0.0), cb = kRkB[stage] * s->dt;
     const int scur = slot(Lcur, it), spre = slot(LP, it), send = slot(LE, it);
     const int sout = Lout >= 0 ? slot(Lout, it) : -1;
+    size_t toff[MAXF] = {};
+    if (trac) trac_slices(s, toff);
     int n = 0;
     for (auto &F : s->faults) {
+      const size_t myoff = toff[n];
       FaultArgs &a = fa[n++];
       a = FaultArgs{};
       a.g = s->g; a.F = F.d;
@@ -226,7 +298,7 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       a.ca = ca; a.cb = cb; a.rkb = kRkB[stage]; a.dt = s->dt;
       a.isfree = s->isfree; a.imethod = s->imethod;
       a.j0 = F.j0; a.k0 = F.k0; a.nj = F.nj; a.nk = F.nk; a.ctl = s->ctl;
-      a.trac = trac ? trac : F.trac; a.tj0 = F.j0 + NG - 3; a.tk0 = F.k0 + NG - 3; a.tnj = F.nj + 6; a.tnk = F.nk + 6;
+      a.trac = trac ? trac + myoff : F.trac; a.tj0 = F.j0 + NG - 3; a.tk0 = F.k0 + NG - 3; a.tnj = F.nj + 6; a.tnk = F.nk + 6;
       if (F.nj > 0 && F.nk > 0) {
         a.wj0 = std::max(0, F.j0 - 3); a.wk0 = std::max(0, F.k0 - 3);
         a.wnj = std::min(s->g.nj - 1, F.j0 + F.nj + 2) - a.wj0 + 1;
@@ -245,8 +317,12 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
   // read only the fault's neighbourhood, away from every PML slab and
   // edge box) start on the fault stream once this stage's interior,
   // surface-row and fault kernels are done, beside its PML and edge kernels.
-  const bool br = s->branches == 1, br2 = s->branches == 2;
+  // branches 3: as 2, and the y and z PML slab kernels run on a third
+  // stream beside the x slab, edge and surface-row kernels (disjoint
+  // points, the same input), so that their launch gaps and tails overlap
+  const bool br = s->branches == 1, br2 = s->branches >= 2, br3 = s->branches == 3;
   const bool early = br2 && s->pre_early;
+  const bool ov = br2 && s->pre_overlap;
   FaultArgs fargs[MAXF], fnext[MAXF];
   const int nfa = stage_fargs(0, fargs);
   for (int stage = 0; stage < 4; stage++) {
@@ -254,15 +330,25 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     const int mode = stage == 0 ? RK_FIRST : (stage == 3 ? RK_LAST : RK_MID);
     const int Lcur = stage == 0 ? LP : (stage == 2 ? LB : LA);
     const int Lout = stage == 0 ? LA : (stage == 1 ? LB : (stage == 2 ? LA : -1));
-    const float ca = stage < 3 ? kRkA[stage] * s->dt : 0.f, cb = kRkB[stage] * s->dt;
+    const real ca = stage < 3 ? kRkA[stage] * s->dt : RL(0.0), cb = kRkB[stage] * s->dt;
     const int scur = slot(Lcur, it), spre = slot(LP, it), send = slot(LE, it);
     const int sout = Lout >= 0 ? slot(Lout, it) : -1;
     if (stage > 0) {
       if (early) std::memcpy(fargs, fnext, sizeof(FaultArgs) * nfa);
       else stage_fargs(stage, fargs);
     }
-    if (!(early && stage > 0))
-      for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fargs[f], s->stream);
+    if (!(early && stage > 0)) {
+      if (ov) {
+        // on the fault stream, beside the interior kernel (which defers the
+        // fault planes), once the stage input is complete
+        cudaEventRecord(s->ev_stage[stage], s->stream);
+        cudaStreamWaitEvent(s->aux[0], s->ev_stage[stage], 0);
+        for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fargs[f], s->aux[0]);
+      } else {
+        for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fargs[f], s->stream);
+      }
+    }
+    if (ov) cudaEventRecord(s->ev_predone[stage], s->aux[0]);
     // external event nodes when captured, so that the events really fire
     // on every graph replay; the stage interval spans the fork to the join
     if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
@@ -281,6 +367,7 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
     v.coef = s->coef; v.free_mat = s->free_mat;
     v.ca = ca; v.cb = cb; v.isfree = s->isfree;
     v.nfault = (int)s->faults.size();
+    v.defer_i0 = ov ? 1 : 0;
     for (size_t f = 0; f < s->faults.size(); f++) { v.fi0[f] = s->faults[f].d.i0; v.fflag[f] = s->faults[f].flag; }
     for (int q = 0; q < 6; q++) {
       v.pml[q] = s->pml[q].d;
@@ -293,13 +380,23 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       // interior box, single-direction PML slabs, generic shell
       const int kind0 = 0;
       for (int kind = kind0; kind < 6; kind++) {
+        if (kind == 1 && ov) {
+          // the fault planes x = i0 once the stage's first fault kernels
+          // (which refresh the split nodes there) are done
+          cudaStreamWaitEvent(s->stream, s->ev_predone[stage], 0);
+          VolArgs vp = vs;
+          volume_boxes(vp, s->kbox[6], s->nkbox[6], true);
+          if (vp.nbox > 0) { launch_volume_plane(vp, idir, jdir, kdir, mode, s->stream); nl++; }
+        }
         if (kind == 1 && br2) {
           // the interior kernel has been issued alone; the fault kernels
           // now overlap the PML slabs and the shell
           st_fault = s->aux[0];
           cudaEventRecord(s->ev_fork[stage], s->stream);
           cudaStreamWaitEvent(st_fault, s->ev_fork[stage], 0);
+          if (br3) cudaStreamWaitEvent(s->aux[1], s->ev_fork[stage], 0);
           for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
+          if (ov) cudaEventRecord(s->ev_postdone[stage], st_fault);
         }
         if (kind == 2 && early && stage < 3) {
           // the surface rows are issued: the next stage's input is complete
@@ -321,8 +418,8 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
             break;
           case 1: launch_volume_shell(vk, idir, jdir, kdir, mode, st_pml); break;
           case 2: launch_volume_face_x(vk, idir, jdir, kdir, mode, st_pml); break;
-          case 3: launch_volume_face_y(vk, idir, jdir, kdir, mode, st_pml); break;
-          case 4: launch_volume_face_z(vk, idir, jdir, kdir, mode, st_pml); break;
+          case 3: launch_volume_face_y(vk, idir, jdir, kdir, mode, br3 ? s->aux[1] : st_pml); break;
+          case 4: launch_volume_face_z(vk, idir, jdir, kdir, mode, br3 ? s->aux[1] : st_pml); break;
           default: launch_volume_edge(vk, idir, jdir, kdir, mode, st_pml); break;
         }
         nl += vk.nbox > 0;
@@ -334,8 +431,19 @@ void enqueue_step(cgfd_solver *s, int it, float *trac = nullptr, bool timed = tr
       cudaStreamWaitEvent(s->stream, s->ev_join[stage][0], 0);
       cudaStreamWaitEvent(s->stream, s->ev_join[stage][1], 0);
     } else if (br2) {
-      cudaEventRecord(s->ev_join[stage][0], st_fault);
-      cudaStreamWaitEvent(s->stream, s->ev_join[stage][0], 0);
+      // with the fault planes deferred, the stage ends when the fault slab
+      // kernels end: the next stage's early first fault kernels, queued
+      // behind them, only have to end before its PLANE launch
+      if (ov) {
+        cudaStreamWaitEvent(s->stream, s->ev_postdone[stage], 0);
+      } else {
+        cudaEventRecord(s->ev_join[stage][0], st_fault);
+        cudaStreamWaitEvent(s->stream, s->ev_join[stage][0], 0);
+      }
+      if (br3) {
+        cudaEventRecord(s->ev_join[stage][1], s->aux[1]);
+        cudaStreamWaitEvent(s->stream, s->ev_join[stage][1], 0);
+      }
     }
     if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][1], s->stream, cudaEventRecordExternal);
   }
@@ -446,10 +554,11 @@ int cgfd_setup_coords(const cgfd_setup *su, float *x, float *y, float *z) {
 int cgfd_setup_bytes(const cgfd_setup *su, unsigned long long *bytes) {
   if (!su || !bytes) return fail(CGFD_ERR_ARG, "bad argument");
   const HostSetup &H = su->H;
-  unsigned long long n = (su->coef_size() + H.free_mat.size()) * 4ull;
-  for (int d = 0; d < 3; d++) for (int q = 0; q < 2; q++) n += 3ull * (H.pml[d][q].A.size()) * 4;
-  for (auto &F : H.faults) n += F.flag.size() + (F.mat.size() + F.fmat.size() + F.scal.size() + F.out.size()) * 4ull;
-  n += H.sta_idx.size() * sizeof(long) + (H.sta_w.size() + H.fsta_w.size()) * 4ull + (H.fsta_fid.size() + H.fsta_idx.size()) * 4ull;
+  const unsigned long long R = sizeof(real);
+  unsigned long long n = (su->coef_size() + H.free_mat.size()) * R;
+  for (int d = 0; d < 3; d++) for (int q = 0; q < 2; q++) n += 3ull * (H.pml[d][q].A.size()) * R;
+  for (auto &F : H.faults) n += F.flag.size() + (F.mat.size() + F.fmat.size() + F.scal.size() + F.out.size()) * R;
+  n += H.sta_idx.size() * sizeof(long) + (H.sta_w.size() + H.fsta_w.size()) * R + (H.fsta_fid.size() + H.fsta_idx.size()) * 4ull;
   *bytes = n;
   return CGFD_OK;
 }
@@ -553,13 +662,13 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   for (int L = 0; L < 4; L++) CK(dalloc(s, &s->w[L], lev), "wavefield");
   CK(dalloc(s, &s->coef, 13 * (size_t)g.scmp), "metric");
   CK(dalloc(s, &s->free_mat, H.free_mat.size()), "free surface");
-  CK(cudaMemcpyAsync(s->coef, su->coef(), su->coef_size() * 4, cudaMemcpyHostToDevice, s->stream), "copy metric");
-  CK(cudaMemcpyAsync(s->free_mat, H.free_mat.data(), H.free_mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy free");
+  CK(to_device(s->coef, su->coef(), su->coef_size(), s->stream), "copy metric");
+  CK(to_device(s->free_mat, H.free_mat.data(), H.free_mat.size(), s->stream), "copy free");
   if (H.abl_nblk > 0) {
     CK(dalloc(s, &s->abl_E, (size_t)g.nx + g.ny + g.nz), "sponge");
-    CK(cudaMemcpyAsync(s->abl_E, H.abl_E[0].data(), g.nx * 4, cudaMemcpyHostToDevice, s->stream), "copy sponge");
-    CK(cudaMemcpyAsync(s->abl_E + g.nx, H.abl_E[1].data(), g.ny * 4, cudaMemcpyHostToDevice, s->stream), "copy sponge");
-    CK(cudaMemcpyAsync(s->abl_E + g.nx + g.ny, H.abl_E[2].data(), g.nz * 4, cudaMemcpyHostToDevice, s->stream), "copy sponge");
+    CK(to_device(s->abl_E, H.abl_E[0].data(), g.nx, s->stream), "copy sponge");
+    CK(to_device(s->abl_E + g.nx, H.abl_E[1].data(), g.ny, s->stream), "copy sponge");
+    CK(to_device(s->abl_E + g.nx + g.ny, H.abl_E[2].data(), g.nz, s->stream), "copy sponge");
     SpongeArgs &sp = s->sponge;
     sp.g = g; sp.E = s->abl_E; sp.nblk = H.abl_nblk;
     sp.first[0] = 0;
@@ -587,7 +696,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     std::copy(P.A.begin(), P.A.end(), cf.begin());
     std::copy(P.B.begin(), P.B.end(), cf.begin() + np);
     std::copy(P.D.begin(), P.D.end(), cf.begin() + 2 * np);
-    CK(cudaMemcpyAsync(S.coef, cf.data(), cf.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy pml");
+    CK(to_device(S.coef, cf.data(), cf.size(), s->stream), "copy pml");
     S.d.A = S.coef; S.d.B = S.coef + np; S.d.D = S.coef + 2 * np;
     for (int L = 0; L < 4; L++) CK(dalloc(s, &S.aux[L], (size_t)NCMP * S.d.siz), "pml aux");
   }
@@ -601,10 +710,10 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     CK(dalloc(s, &F.scal, Fh.scal.size()), "fault scalars");
     CK(dalloc(s, &F.out, Fh.out.size()), "fault output");
     CK(cudaMemcpyAsync(F.flag, Fh.flag.data(), ns, cudaMemcpyHostToDevice, s->stream), "copy");
-    CK(cudaMemcpyAsync(F.mat, Fh.mat.data(), Fh.mat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
-    CK(cudaMemcpyAsync(F.fmat, Fh.fmat.data(), Fh.fmat.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
-    CK(cudaMemcpyAsync(F.scal, Fh.scal.data(), Fh.scal.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
-    CK(cudaMemcpyAsync(F.out, Fh.out.data(), Fh.out.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(to_device(F.mat, Fh.mat.data(), Fh.mat.size(), s->stream), "copy");
+    CK(to_device(F.fmat, Fh.fmat.data(), Fh.fmat.size(), s->stream), "copy");
+    CK(to_device(F.scal, Fh.scal.data(), Fh.scal.size(), s->stream), "copy");
+    CK(to_device(F.out, Fh.out.data(), Fh.out.size(), s->stream), "copy");
     F.d.i0 = Fh.i0; F.d.bit = 1 << f; F.d.flag_in = F.flag; F.d.flag = F.flag;
     F.d.mat = F.mat; F.d.fmat = F.fmat; F.d.scal = F.scal; F.d.out = F.out;
     int j0 = g.nj, j1 = -1, k0 = g.nk, k1 = -1;
@@ -631,12 +740,12 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   CK(dalloc(s, &s->fseis, (size_t)st.nf * 9 * std::max(1, st.max_rec)), "fault seismograms");
   if (!H.sta_idx.empty()) {
     CK(cudaMemcpyAsync(s->sta_idx, H.sta_idx.data(), H.sta_idx.size() * sizeof(long), cudaMemcpyHostToDevice, s->stream), "copy");
-    CK(cudaMemcpyAsync(s->sta_w, H.sta_w.data(), H.sta_w.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(to_device(s->sta_w, H.sta_w.data(), H.sta_w.size(), s->stream), "copy");
   }
   if (!H.fsta_fid.empty()) {
     CK(cudaMemcpyAsync(s->fsta_fid, H.fsta_fid.data(), H.fsta_fid.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
     CK(cudaMemcpyAsync(s->fsta_idx, H.fsta_idx.data(), H.fsta_idx.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
-    CK(cudaMemcpyAsync(s->fsta_w, H.fsta_w.data(), H.fsta_w.size() * 4, cudaMemcpyHostToDevice, s->stream), "copy");
+    CK(to_device(s->fsta_w, H.fsta_w.data(), H.fsta_w.size(), s->stream), "copy");
   }
   st.idx = s->sta_idx; st.w = s->sta_w; st.fid = s->fsta_fid; st.fidx = s->fsta_idx; st.fw = s->fsta_w;
   st.seis = s->seis; st.fseis = s->fseis;
@@ -694,6 +803,15 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     }
     const char *pe = std::getenv("CGFD_PRE_EARLY");
     if (pe && pe[0] == '0') s->pre_early = false;
+    // the fault planes inside the interior box, for the PLANE launch when
+    // the interior kernel defers them
+    for (auto &F : s->faults) {
+      const int ii = F.d.i0 - NG;
+      if (ii >= ilo && ii <= ihi) add(6, ii, ii, jlo, jhi, klo, khi);
+    }
+    s->pre_overlap = !s->faults.empty();
+    const char *po = std::getenv("CGFD_PRE_OVERLAP");
+    if (po && po[0] == '0') s->pre_overlap = false;
     const char *pk = std::getenv("CGFD_PACK");
     if (pk && pk[0] == '0') s->pack = false;
     // y tiles (8 rows) per interior chunk: the z window of a chunk, about 8
@@ -723,6 +841,15 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
         }
       }
     }
+    // the fault planes deferred to the PLANE launch (welded nodes; the split
+    // nodes belong to the fault kernels)
+    if (s->pre_overlap)
+      for (size_t f = 0; f < H.faults.size(); f++) {
+        const int i = H.faults[f].i0 - NG;
+        if (i < ilo || i > ihi) continue;
+        for (int k = klo; k <= khi; k++) for (int j = jlo; j <= jhi; j++)
+          if (!(H.faults[f].flag[(size_t)(j + NG) + (size_t)(k + NG) * g.ny] & FL_SPLIT)) nint--;
+      }
     s->int_points = nint;
     s->vol_points = nall;
   }
@@ -739,6 +866,9 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     if (br) s->branches = std::atoi(br);
     for (int q = 0; q < 3; q++) CK(cudaStreamCreateWithFlags(&s->aux[q], cudaStreamNonBlocking), "stream");
     for (int a = 0; a < 4; a++) {
+      CK(cudaEventCreateWithFlags(&s->ev_stage[a], cudaEventDisableTiming), "event");
+      CK(cudaEventCreateWithFlags(&s->ev_predone[a], cudaEventDisableTiming), "event");
+      CK(cudaEventCreateWithFlags(&s->ev_postdone[a], cudaEventDisableTiming), "event");
       CK(cudaEventCreateWithFlags(&s->ev_fork[a], cudaEventDisableTiming), "event");
       CK(cudaEventCreateWithFlags(&s->ev_pre[a], cudaEventDisableTiming), "event");
       for (int b = 0; b < 3; b++) CK(cudaEventCreateWithFlags(&s->ev_join[a][b], cudaEventDisableTiming), "event");
@@ -867,11 +997,103 @@ int cgfd_run(cgfd_solver *s, int nsteps) {
   return CGFD_OK;
 }
 
+// ---- cgfd_run_fault_output ----------------------------------------------------
+
+int cgfd_run_fault_output(cgfd_solver *s, int nsteps, int every, float *out, long long max_records, int *nrec) {
+  if (!s || nsteps < 0 || every < 1 || max_records < 0) return fail(CGFD_ERR_ARG, "bad argument");
+  const Grid &g = s->g;
+  const int nf = (int)s->faults.size();
+  const size_t fsz = (size_t)CGFD_FAULT_NFIELD * g.nj * g.nk, rsz = fsz * nf;
+  long long want = 0;
+  for (int q = 0; q < nsteps; q++) want += (s->it + q) % every == 0;
+  if (want > max_records) return fail(CGFD_ERR_ARG, "output buffer holds fewer records than the run takes");
+  if (want > 0 && (!out || nf == 0)) return fail(CGFD_ERR_ARG, "no output buffer, or no fault");
+  if (nrec) *nrec = 0;
+  cudaError_t e = cudaSuccess;
+  if (want > 0 && !s->rec_buf[0]) {
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) e = dalloc(s, &s->rec_buf[b], rsz);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+      e = cudaEventCreateWithFlags(&s->ev_gathered[b], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_copied[b], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "fault output staging");
+  }
+  long long nl = 0, rec = 0;
+  e = cudaEventRecord(s->ev_run[0], s->stream);
+  for (int q = 0; q < nsteps && e == cudaSuccess; q++) {
+    const int it = s->it;
+    if (it % every == 0) {
+      // gather into the staging buffer of this record's parity once its
+      // previous copy has left it, then copy it out on the copy stream
+      // while the next steps run
+      const int b = (int)(rec & 1);
+      if (rec >= 2) e = cudaStreamWaitEvent(s->stream, s->ev_copied[b], 0);
+      for (int f = 0; f < nf && e == cudaSuccess; f++) {
+        launch_fault_gather(s->faults[f].out, s->rec_buf[b] + f * fsz, CGFD_FAULT_NFIELD, g, s->stream);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(s->ev_gathered[b], s->stream);
+#ifdef CGFD_FP64
+      if (e == cudaSuccess) e = to_host(out + rec * rsz, s->rec_buf[b], rsz, s->stream);
+#else
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy, s->ev_gathered[b], 0);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out + rec * rsz, s->rec_buf[b], rsz * sizeof(real), cudaMemcpyDeviceToHost, s->copy);
+      if (e == cudaSuccess) e = cudaEventRecord(s->ev_copied[b], s->copy);
+#endif
+      rec++;
+      nl += nf;
+    }
+    if (e != cudaSuccess) break;
+    if (s->use_graph) {
+      cudaGraphExec_t &G = s->graph[s->timing][it % 8];
+      if (!G) {
+        const int rc = build_graph(s, it);
+        if (rc != CGFD_OK) return rc;
+      }
+      e = cudaGraphLaunch(G, s->stream);
+    } else {
+      enqueue_step(s, it);
+      e = cudaGetLastError();
+    }
+    nl += s->launches_per_step;
+    s->it++;
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(s->ev_run[1], s->stream);
+  if (e == cudaSuccess && s->copy) e = cudaStreamSynchronize(s->copy);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "run with fault output");
+  if (nrec) *nrec = (int)rec;
+  float run_ms = 0;
+  cudaEventElapsedTime(&run_ms, s->ev_run[0], s->ev_run[1]);
+  s->run_ms = run_ms; s->vol_ms = s->int_ms = 0; s->vol_launches = s->int_launches = 0;
+  s->last_launches = nl;
+  Ctl c;
+  e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "read control block");
+  if (c.it != s->it) return fail(CGFD_ERR_STATE, "device step counter out of step with the host");
+  if (c.err & CTL_ERR_NONFINITE) return fail(CGFD_ERR_UNSTABLE, "non-finite slip rate or station value");
+  return CGFD_OK;
+}
+
+int cgfd_host_alloc(unsigned long long bytes, void **ptr) {
+  if (!ptr) return fail(CGFD_ERR_ARG, "bad argument");
+  *ptr = nullptr;
+  const cudaError_t e = cudaMallocHost(ptr, std::max<unsigned long long>(bytes, 1));
+  if (e != cudaSuccess) { *ptr = nullptr; return cuda_fail(e, "page-locked host memory"); }
+  return CGFD_OK;
+}
+
+void cgfd_host_free(void *ptr) {
+  if (ptr) cudaFreeHost(ptr);
+}
+
 // ---- cgfd_run_noalloc ------------------------------------------------------
 
 namespace {
 constexpr int kNoallocMaxDevices = 64;
-std::atomic<float *> g_noalloc_ptr[kNoallocMaxDevices];
+std::atomic<real *> g_noalloc_ptr[kNoallocMaxDevices];
 
 int fail_fixed(int code, const char *m) {
   size_t n = 0;
@@ -890,29 +1112,29 @@ int fail_fixed_cuda(cudaError_t e, const char *what) {
 
 int cgfd_run_noalloc(cgfd_solver *s, int nsteps) {
   if (!s || nsteps < 0) return fail_fixed(CGFD_ERR_ARG, "bad argument");
-  // the largest fault's traction scratch must fit the static array
-  for (const FaultState &F : s->faults) {
-    if (F.nj <= 0 || F.nk <= 0) continue;
-    const unsigned long long need = 12ull * 9 * (F.nj + 6) * (F.nk + 6);
-    if (need > CGFD_NOALLOC_SCRATCH_FLOATS) {
-      char b[sizeof g_err_fixed];
-      std::snprintf(b, sizeof b,
-                    "cgfd_run_noalloc: the fault's split box needs %llu scratch floats, the static array holds %u",
-                    need, CGFD_NOALLOC_SCRATCH_FLOATS);
-      return fail_fixed(CGFD_ERR_ARG, b);
-    }
+  // every fault takes its own slice of the static array: their sum must fit
+  size_t toff[MAXF];
+  const unsigned long long need = trac_slices(s, toff);
+  if (need > CGFD_NOALLOC_SCRATCH_FLOATS) {
+    char b[sizeof g_err_fixed];
+    std::snprintf(b, sizeof b,
+                  "cgfd_run_noalloc: the faults' split boxes need %llu scratch floats together, the static array holds %u",
+                  need, CGFD_NOALLOC_SCRATCH_FLOATS);
+    return fail_fixed(CGFD_ERR_ARG, b);
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: current device");
   if (dev < 0 || dev >= kNoallocMaxDevices) return fail_fixed(CGFD_ERR_ARG, "cgfd_run_noalloc: device ordinal too large");
-  float *trac = g_noalloc_ptr[dev].load();
+  real *trac = g_noalloc_ptr[dev].load();
   if (!trac) {
     e = noalloc_scratch_address(&trac);
     if (e != cudaSuccess) return fail_fixed_cuda(e, "cgfd_run_noalloc: scratch address");
     g_noalloc_ptr[dev].store(trac);
   }
   long long nl = 0;
+  s->run_ms = s->vol_ms = s->int_ms = 0;
+  s->vol_launches = s->int_launches = 0;
   for (int q = 0; q < nsteps; q++) {
     enqueue_step(s, s->it, trac, false);
     e = cudaGetLastError();
@@ -1064,11 +1286,7 @@ int cgfd_get_fault_all(cgfd_solver *s, int f, float *out) {
   // gather the interior nodes on the device, then one contiguous copy
   launch_fault_gather(s->faults[f].out, s->faults[f].gather, CGFD_FAULT_NFIELD, g, s->stream);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(out, s->faults[f].gather, (size_t)CGFD_FAULT_NFIELD * g.nj * g.nk * 4,
-                        cudaMemcpyDeviceToHost, s->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "read fault");
-  e = cudaStreamSynchronize(s->stream);
+  if (e == cudaSuccess) e = to_host(out, s->faults[f].gather, (size_t)CGFD_FAULT_NFIELD * g.nj * g.nk, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read fault");
   return CGFD_OK;
 }
@@ -1079,14 +1297,13 @@ int cgfd_get_fault(cgfd_solver *s, int f, int field, float *out) {
   const Grid &g = s->g;
   const size_t ns = (size_t)g.ny * g.nz;
   std::vector<float> h(ns);
-  cudaError_t e = cudaMemcpyAsync(h.data(), s->faults[f].out + field * ns, ns * 4, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaError_t e = to_host(h.data(), s->faults[f].out + field * ns, ns, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read fault");
   for (int k = 0; k < g.nk; k++) std::memcpy(out + (size_t)k * g.nj, h.data() + (size_t)(k + NG) * g.ny + NG, (size_t)g.nj * 4);
   return CGFD_OK;
 }
 
-static int get_series(cgfd_solver *s, float *dev, int n, float *out, int *nrec) {
+static int get_series(cgfd_solver *s, real *dev, int n, float *out, int *nrec) {
   Ctl c;
   cudaError_t e = cudaMemcpy(&c, s->ctl, sizeof c, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read control block");
@@ -1094,7 +1311,7 @@ static int get_series(cgfd_solver *s, float *dev, int n, float *out, int *nrec) 
   if (!out || n == 0 || c.nrec == 0) return CGFD_OK;
   const int mr = s->st.max_rec;
   std::vector<float> h((size_t)n * 9 * mr);
-  e = cudaMemcpy(h.data(), dev, h.size() * 4, cudaMemcpyDeviceToHost);
+  e = to_host(h.data(), dev, h.size(), s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read series");
   for (size_t q = 0; q < (size_t)n * 9; q++) std::memcpy(out + q * c.nrec, h.data() + q * mr, (size_t)c.nrec * 4);
   return CGFD_OK;
@@ -1125,8 +1342,7 @@ int cgfd_get_surface_peaks(cgfd_solver *s, float *out) {
   if (!s || !out) return fail(CGFD_ERR_ARG, "bad argument");
   if (!s->pg) return fail(CGFD_ERR_ARG, "no free surface: no surface peaks");
   const size_t n = (size_t)CGFD_NPEAK * s->g.ni * s->g.nj;
-  cudaError_t e = cudaMemcpyAsync(out, s->pg, n * 4, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaError_t e = to_host(out, s->pg, n, s->stream);
   return e == cudaSuccess ? CGFD_OK : cuda_fail(e, "read surface peaks");
 }
 
@@ -1135,8 +1351,7 @@ int cgfd_get_wavefield(cgfd_solver *s, int cmp, float *out) {
   const Grid &g = s->g;
   const CmpArray A = cmp_array(g, cmp);
   std::vector<float> h(A.n);
-  cudaError_t e = cudaMemcpyAsync(h.data(), s->w[slot(LP, s->it)] + A.off, A.n * 4, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaError_t e = to_host(h.data(), s->w[slot(LP, s->it)] + A.off, A.n, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read wavefield");
   for (int k = 0; k < g.nk; k++)
     for (int j = 0; j < g.nj; j++) {
@@ -1152,8 +1367,8 @@ int cgfd_set_wavefield(cgfd_solver *s, int cmp, const float *in) {
   const Grid &g = s->g;
   const CmpArray A = cmp_array(g, cmp);
   std::vector<float> h(A.n);
-  float *dst = s->w[slot(LP, s->it)] + A.off;
-  cudaError_t e = cudaMemcpy(h.data(), dst, A.n * 4, cudaMemcpyDeviceToHost);
+  real *dst = s->w[slot(LP, s->it)] + A.off;
+  cudaError_t e = to_host(h.data(), dst, A.n, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "read wavefield");
   for (int k = 0; k < g.nk; k++)
     for (int j = 0; j < g.nj; j++) {
@@ -1161,7 +1376,8 @@ int cgfd_set_wavefield(cgfd_solver *s, int cmp, const float *in) {
       const float *src = in + ((size_t)k * g.nj + j) * g.ni;
       for (int i = 0; i < g.ni; i++) d[(size_t)i * A.step] = src[i];
     }
-  e = cudaMemcpy(dst, h.data(), A.n * 4, cudaMemcpyHostToDevice);
+  e = to_device(dst, h.data(), A.n, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "write wavefield");
   return CGFD_OK;
 }
@@ -1174,19 +1390,19 @@ static std::vector<std::pair<void *, size_t>> state_parts(cgfd_solver *s) {
   const size_t ns = (size_t)g.ny * g.nz;
   const int sp = slot(LP, s->it);
   v.push_back({ s->ctl, sizeof(Ctl) });
-  v.push_back({ s->w[sp], (size_t)NCMP * g.scmp * 4 });
-  for (int q = 0; q < 6; q++) if (s->pml[q].d.on) v.push_back({ s->pml[q].aux[sp], (size_t)NCMP * s->pml[q].d.siz * 4 });
+  v.push_back({ s->w[sp], (size_t)NCMP * g.scmp * sizeof(real) });
+  for (int q = 0; q < 6; q++) if (s->pml[q].d.on) v.push_back({ s->pml[q].aux[sp], (size_t)NCMP * s->pml[q].d.siz * sizeof(real) });
   for (auto &F : s->faults) {
-    v.push_back({ F.lev[sp], 18 * ns * 4 });
-    v.push_back({ F.scal, (size_t)NFS * ns * 4 });
-    v.push_back({ F.out, (size_t)CGFD_FAULT_NFIELD * ns * 4 });
+    v.push_back({ F.lev[sp], 18 * ns * sizeof(real) });
+    v.push_back({ F.scal, (size_t)NFS * ns * sizeof(real) });
+    v.push_back({ F.out, (size_t)CGFD_FAULT_NFIELD * ns * sizeof(real) });
     v.push_back({ F.flag, ns });
   }
-  v.push_back({ s->seis, (size_t)s->st.n * 9 * std::max(1, s->st.max_rec) * 4 });
-  v.push_back({ s->fseis, (size_t)s->st.nf * 9 * std::max(1, s->st.max_rec) * 4 });
+  v.push_back({ s->seis, (size_t)s->st.n * 9 * std::max(1, s->st.max_rec) * sizeof(real) });
+  v.push_back({ s->fseis, (size_t)s->st.nf * 9 * std::max(1, s->st.max_rec) * sizeof(real) });
   if (s->pg) {
-    v.push_back({ s->pg, (size_t)CGFD_NPEAK * g.ni * g.nj * 4 });
-    v.push_back({ s->dis, (size_t)3 * g.ni * g.nj * 4 });
+    v.push_back({ s->pg, (size_t)CGFD_NPEAK * g.ni * g.nj * sizeof(real) });
+    v.push_back({ s->dis, (size_t)3 * g.ni * g.nj * sizeof(real) });
   }
   return v;
 }

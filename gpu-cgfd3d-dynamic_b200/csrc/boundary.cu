@@ -25,14 +25,14 @@ __global__ void __launch_bounds__(256) k_sponge(const SpongeArgs a) {
   const int ni = B[1] - B[0] + 1, nj = B[3] - B[2] + 1;
   const int i = B[0] + (int)(u % ni), j = B[2] + (int)((u / ni) % nj), k = B[4] + (int)(u / ((long)ni * nj));
   const Grid &g = a.g;
-  const float ex = __ldg(a.E + i), ey = __ldg(a.E + g.nx + j), ez = __ldg(a.E + g.nx + g.ny + k);
+  const real ex = __ldg(a.E + i), ey = __ldg(a.E + g.nx + j), ez = __ldg(a.E + g.nx + g.ny + k);
   // the reference's selection order: min(Ex, Ey), then Ez
-  float mask = ex < ey ? ex : ey;
+  real mask = ex < ey ? ex : ey;
   if (mask > ez) mask = ez;
   const long p = g.at(i, j, k), sc = g.scmp;
-  float4 *A = reinterpret_cast<float4 *>(a.w) + p, *Bq = reinterpret_cast<float4 *>(a.w + 4 * sc) + p;
-  float4 x = *A, y = *Bq;
-  float tz = a.w[8 * sc + p];
+  real4 *A = reinterpret_cast<real4 *>(a.w) + p, *Bq = reinterpret_cast<real4 *>(a.w + 4 * sc) + p;
+  real4 x = *A, y = *Bq;
+  real tz = a.w[8 * sc + p];
   x.x *= mask; x.y *= mask; x.z *= mask; x.w *= mask;
   y.x *= mask; y.y *= mask; y.z *= mask; y.w *= mask;
   *A = x; *Bq = y;
@@ -46,26 +46,26 @@ __global__ void __launch_bounds__(256) k_surface_peaks(const PeakArgs a) {
   if (i >= g.ni || j >= g.nj) return;
   const long p = g.at(i + NG, j + NG, g.nk + NG - 1);
   // velocities are the first three lanes of the first 16-byte group
-  const float4 v1 = __ldg(reinterpret_cast<const float4 *>(a.wend) + p);
-  const float4 v0 = __ldg(reinterpret_cast<const float4 *>(a.wpre) + p);
+  const real4 v1 = __ldg(reinterpret_cast<const real4 *>(a.wend) + p);
+  const real4 v0 = __ldg(reinterpret_cast<const real4 *>(a.wpre) + p);
   const long n = (long)g.ni * g.nj, q = i + (long)j * g.ni;
-  const float dt = a.dt;
-  const float Ax = fabsf((v1.x - v0.x) / dt), Ay = fabsf((v1.y - v0.y) / dt), Az = fabsf((v1.z - v0.z) / dt);
+  const real dt = a.dt;
+  const real Ax = fabs((v1.x - v0.x) / dt), Ay = fabs((v1.y - v0.y) / dt), Az = fabs((v1.z - v0.z) / dt);
   // displacement by the trapezoid rule, accumulated through double as in
   // the reference (its 0.5 is a double constant)
-  float Dx = a.dis[q], Dy = a.dis[n + q], Dz = a.dis[2 * n + q];
+  real Dx = a.dis[q], Dy = a.dis[n + q], Dz = a.dis[2 * n + q];
   Dx += 0.5 * (v1.x + v0.x) * dt;
   Dy += 0.5 * (v1.y + v0.y) * dt;
   Dz += 0.5 * (v1.z + v0.z) * dt;
   a.dis[q] = Dx; a.dis[n + q] = Dy; a.dis[2 * n + q] = Dz;
-  const float val[15] = {
-      sqrtf(v1.x * v1.x + v1.y * v1.y + v1.z * v1.z), sqrtf(v1.x * v1.x + v1.y * v1.y),
-      fabsf(v1.x), fabsf(v1.y), fabsf(v1.z),
-      sqrtf(Ax * Ax + Ay * Ay + Az * Az), sqrtf(Ax * Ax + Ay * Ay), Ax, Ay, Az,
-      sqrtf(Dx * Dx + Dy * Dy + Dz * Dz), sqrtf(Dx * Dx + Dy * Dy), fabsf(Dx), fabsf(Dy), fabsf(Dz) };
+  const real val[15] = {
+      sqrt(v1.x * v1.x + v1.y * v1.y + v1.z * v1.z), sqrt(v1.x * v1.x + v1.y * v1.y),
+      fabs(v1.x), fabs(v1.y), fabs(v1.z),
+      sqrt(Ax * Ax + Ay * Ay + Az * Az), sqrt(Ax * Ax + Ay * Ay), Ax, Ay, Az,
+      sqrt(Dx * Dx + Dy * Dy + Dz * Dz), sqrt(Dx * Dx + Dy * Dy), fabs(Dx), fabs(Dy), fabs(Dz) };
 #pragma unroll
   for (int c = 0; c < 15; c++) {
-    float *o = a.pg + c * n + q;
+    real *o = a.pg + c * n + q;
     if (*o < val[c]) *o = val[c];
   }
 }

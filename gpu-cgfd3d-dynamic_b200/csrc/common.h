@@ -17,6 +17,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "real.h"
+
 #ifdef __CUDACC__
 #define CGFD_HD __host__ __device__
 #else
@@ -41,10 +43,10 @@ enum Met { MJAC = 0, MXIX, MXIY, MXIZ, METX, METY, METZ, MZTX, MZTY, MZTZ };
 // one medium value: (xi_x xi_y xi_z lambda), (eta_x eta_y eta_z mu),
 // (zeta_x zeta_y zeta_z 1/rho).
 #ifdef __CUDACC__
-__device__ __forceinline__ float4 coef_row(const float *cf, long scmp, int d, long q) {
-  return __ldg(reinterpret_cast<const float4 *>(cf + scmp) + d * scmp + q);
+__device__ __forceinline__ real4 coef_row(const real *cf, long scmp, int d, long q) {
+  return __ldg(reinterpret_cast<const real4 *>(cf + scmp) + d * scmp + q);
 }
-__device__ __forceinline__ float coef_jac(const float *cf, long q) { return __ldg(cf + q); }
+__device__ __forceinline__ real coef_jac(const real *cf, long q) { return __ldg(cf + q); }
 #endif
 
 // per-node 3x3 fault matrices, [NFM][nodes][9]
@@ -96,12 +98,12 @@ struct PmlFaceDev {
   int i1, j1, k1;        // first point of the face region (ghost-inclusive indices)
   int fni, fnj, fnk;     // face region extents
   long siz;              // fni*fnj*fnk
-  const float *A, *B, *D;   // per layer along the normal
+  const real *A, *B, *D;   // per layer along the normal
   // auxiliary-field levels used by one stage (9*siz floats each, grouped
   // like a wavefield level with siz points per component): stage input,
   // time-n level, next-stage output, end accumulator
-  const float *acur, *apre;
-  float *aout, *aend;
+  const real *acur, *apre;
+  real *aout, *aend;
 };
 
 struct FaultDev {
@@ -109,21 +111,21 @@ struct FaultDev {
   int bit;
   const uint8_t *flag_in;   // FL_SPLIT / FL_RUPY / FL_RUPZ / FL_GRID per node [ny*nz]
   uint8_t *flag;            // mutable flags (FL_T0SET, FL_RUP)
-  const float *mat;         // [NFM][ny*nz][9]
-  const float *fmat;        // [NFF][ny][9]
-  float *scal;              // [NFS][ny*nz]
-  float *out;               // [11][ny*nz] Tn..Init_t0
+  const real *mat;         // [NFM][ny*nz][9]
+  const real *fmat;        // [NFF][ny][9]
+  real *scal;              // [NFS][ny*nz]
+  real *out;               // [11][ny*nz] Tn..Init_t0
 };
 
 struct StationDev {
   int n, nf, max_rec;
   const long *idx;          // [n][8] volume indices (corner 4 unused: reference quirk)
-  const float *w;           // [n][3] di, dj, dk
+  const real *w;           // [n][3] di, dj, dk
   const int *fid;           // [nf] fault id
   const int *fidx;          // [nf][4] node indices
-  const float *fw;          // [nf][2] dj, dk
-  float *seis;              // [n][9][max_rec]
-  float *fseis;             // [nf][9][max_rec]
+  const real *fw;          // [nf][2] dj, dk
+  real *seis;              // [n][9][max_rec]
+  real *fseis;             // [nf][9][max_rec]
 };
 
 // control block in device memory, advanced on the device so that a step

@@ -24,7 +24,7 @@
 // last (prefetch), and interior threads for the next z row's DRAM misses.
 //
 // A level stores the nine components of a point in two 16-byte groups and
-// one float (Grid::w), so a stencil tap is three loads: x taps are
+// one real (Grid::w), so a stencil tap is three loads: x taps are
 // immediate offsets from three base pointers, y / z taps share two int
 // offset tables, the centre sample is loaded once for all three
 // directions.  The RHS is built direction by direction, so a PML face of
@@ -46,13 +46,13 @@ constexpr int BX = 32, BY = 8;
 // conservative traction J * (e . sigma_row) at point q for metric row d
 // (0: xi, 1: eta, 2: zeta), all three stress rows (xx,xy,xz), (xy,yy,yz),
 // (xz,yz,zz)
-__device__ __forceinline__ void ctrac3(const Grid &g, const float *__restrict__ w, const float *__restrict__ cf,
-                                       long q, int d, float t[3]) {
-  const float4 e = coef_row(cf, g.scmp, d, q);
-  const float J = coef_jac(cf, q);
-  const float sxx = __ldg(w + g.w(TXX, q)), sxy = __ldg(w + g.w(TXY, q));
-  const float4 s4 = __ldg(reinterpret_cast<const float4 *>(w + 4 * g.scmp) + q);   // Tyy Tzz Tyz Txz
-  const float syy = s4.x, szz = s4.y, syz = s4.z, sxz = s4.w;
+__device__ __forceinline__ void ctrac3(const Grid &g, const real *__restrict__ w, const real *__restrict__ cf,
+                                       long q, int d, real t[3]) {
+  const real4 e = coef_row(cf, g.scmp, d, q);
+  const real J = coef_jac(cf, q);
+  const real sxx = __ldg(w + g.w(TXX, q)), sxy = __ldg(w + g.w(TXY, q));
+  const real4 s4 = __ldg(reinterpret_cast<const real4 *>(w + 4 * g.scmp) + q);   // Tyy Tzz Tyz Txz
+  const real syy = s4.x, szz = s4.y, syz = s4.z, sxz = s4.w;
   t[0] = J * (e.x * sxx + e.y * sxy + e.z * sxz);
   t[1] = J * (e.x * sxy + e.y * syy + e.z * syz);
   t[2] = J * (e.x * sxz + e.y * syz + e.z * szz);
@@ -60,27 +60,27 @@ __device__ __forceinline__ void ctrac3(const Grid &g, const float *__restrict__ 
 
 // the point's three groups within one level
 struct Taps {
-  const float4 *__restrict__ a;  // Vx Vy Vz Txx
-  const float4 *__restrict__ b;  // Tyy Tzz Tyz Txz
-  const float *__restrict__ t;   // Txy
+  const real4 *__restrict__ a;  // Vx Vy Vz Txx
+  const real4 *__restrict__ b;  // Tyy Tzz Tyz Txz
+  const real *__restrict__ t;   // Txy
 };
-__device__ __forceinline__ Taps taps_at(const float *w, long sc, long p) {
+__device__ __forceinline__ Taps taps_at(const real *w, long sc, long p) {
   Taps T;
-  T.a = reinterpret_cast<const float4 *>(w) + p;
-  T.b = reinterpret_cast<const float4 *>(w + 4 * sc) + p;
+  T.a = reinterpret_cast<const real4 *>(w) + p;
+  T.b = reinterpret_cast<const real4 *>(w + 4 * sc) + p;
   T.t = w + 8 * sc + p;
   return T;
 }
 // the nine components of the point o points away
-__device__ __forceinline__ void ld9(const Taps &T, int o, float v[9]) {
-  const float4 x = __ldg(T.a + o), y = __ldg(T.b + o);
+__device__ __forceinline__ void ld9(const Taps &T, int o, real v[9]) {
+  const real4 x = __ldg(T.a + o), y = __ldg(T.b + o);
   v[VX] = x.x; v[VY] = x.y; v[VZ] = x.z; v[TXX] = x.w;
   v[TYY] = y.x; v[TZZ] = y.y; v[TYZ] = y.z; v[TXZ] = y.w;
   v[TXY] = __ldg(T.t + o);
 }
 
 template <int F>
-__device__ __forceinline__ float wdrp(int n) {
+__device__ __forceinline__ real wdrp(int n) {
   return F ? (n == 0 ? kC1 : n == 1 ? kC2 : n == 2 ? kC3 : n == 3 ? kC4 : kC5)
            : (n == 0 ? -kC5 : n == 1 ? -kC4 : n == 2 ? -kC3 : n == 3 ? -kC2 : -kC1);
 }
@@ -92,8 +92,8 @@ __device__ __forceinline__ void tap_offsets(int s, int off[4]) {
 }
 
 // direction-d part of the RHS from the nine d-derivatives D[c] and e = e_d
-__device__ __forceinline__ void rhs_dir(const float D[9], const float e[3], float lam, float mu, float l2m,
-                                        float slw, float r[9]) {
+__device__ __forceinline__ void rhs_dir(const real D[9], const real e[3], real lam, real mu, real l2m,
+                                        real slw, real r[9]) {
   r[VX] = slw * (e[0] * D[TXX] + e[1] * D[TXY] + e[2] * D[TXZ]);
   r[VY] = slw * (e[0] * D[TXY] + e[1] * D[TYY] + e[2] * D[TYZ]);
   r[VZ] = slw * (e[0] * D[TXZ] + e[1] * D[TYZ] + e[2] * D[TZZ]);
@@ -111,8 +111,8 @@ __device__ __forceinline__ void rhs_dir(const float D[9], const float e[3], floa
 // Each tap's nine components come in one go; the sums keep the order of
 // the coefficient table.
 template <int F>
-__device__ __forceinline__ void derivs(const Taps &T, const float v0[9], const int off[4], float D[9]) {
-  float t[9];
+__device__ __forceinline__ void derivs(const Taps &T, const real v0[9], const int off[4], real D[9]) {
+  real t[9];
   ld9(T, off[0], t);
 #pragma unroll
   for (int c = 0; c < 9; c++) D[c] = (F ? kC1 : kC5) * t[c];
@@ -139,13 +139,13 @@ __device__ __forceinline__ void derivs(const Taps &T, const float v0[9], const i
 // gradient G[c][b] = dV_c/dx_b and the momentum sums
 // s_r = sum_a e_a . d(sigma_row r)/dxi_a.
 template <int F>
-__device__ __forceinline__ void acc_dir(const Taps &T, const float v0[9], const int off[4], const float ea[3],
-                                        float G[3][3], float s[3]) {
-  float D[9];
+__device__ __forceinline__ void acc_dir(const Taps &T, const real v0[9], const int off[4], const real ea[3],
+                                        real G[3][3], real s[3]) {
+  real D[9];
   derivs<F>(T, v0, off, D);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const float d = D[VX + c];
+    const real d = D[VX + c];
     G[c][0] += ea[0] * d; G[c][1] += ea[1] * d; G[c][2] += ea[2] * d;
   }
   s[0] += ea[0] * D[TXX];
@@ -158,18 +158,18 @@ __device__ __forceinline__ void acc_dir(const Taps &T, const float v0[9], const 
 
 // the nine components of point p of a level in the grouped layout with
 // sc points per component (read-only data through the non-coherent path)
-__device__ __forceinline__ void ld9(const float *w, long sc, long p, float v[9], bool ro) {
-  const float4 *A = reinterpret_cast<const float4 *>(w) + p, *B = reinterpret_cast<const float4 *>(w + 4 * sc) + p;
-  const float4 x = ro ? __ldg(A) : *A, y = ro ? __ldg(B) : *B;
+__device__ __forceinline__ void ld9(const real *w, long sc, long p, real v[9], bool ro) {
+  const real4 *A = reinterpret_cast<const real4 *>(w) + p, *B = reinterpret_cast<const real4 *>(w + 4 * sc) + p;
+  const real4 x = ro ? __ldg(A) : *A, y = ro ? __ldg(B) : *B;
   v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
   v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
   v[8] = ro ? __ldg(w + 8 * sc + p) : w[8 * sc + p];
 }
 // level value + k * h at point p of level w
-__device__ __forceinline__ void st9(float *w, long sc, long p, const float v[9], float k, const float h[9]) {
-  reinterpret_cast<float4 *>(w)[p] = make_float4(v[0] + k * h[0], v[1] + k * h[1], v[2] + k * h[2], v[3] + k * h[3]);
-  reinterpret_cast<float4 *>(w + 4 * sc)[p] =
-      make_float4(v[4] + k * h[4], v[5] + k * h[5], v[6] + k * h[6], v[7] + k * h[7]);
+__device__ __forceinline__ void st9(real *w, long sc, long p, const real v[9], real k, const real h[9]) {
+  reinterpret_cast<real4 *>(w)[p] = make_real4(v[0] + k * h[0], v[1] + k * h[1], v[2] + k * h[2], v[3] + k * h[3]);
+  reinterpret_cast<real4 *>(w + 4 * sc)[p] =
+      make_real4(v[4] + k * h[4], v[5] + k * h[5], v[6] + k * h[6], v[7] + k * h[7]);
   w[8 * sc + p] = v[8] + k * h[8];
 }
 // L2 prefetch of the auxiliary-field lines that pml_face reads at (I, J, K)
@@ -178,7 +178,7 @@ __device__ __forceinline__ void pml_prefetch(const PmlFaceDev &P, int I, int J, 
   const int li = I - P.i1, lj = J - P.j1, lk = K - P.k1;
   if (li < 0 || li >= P.fni || lj < 0 || lj >= P.fnj || lk < 0 || lk >= P.fnk) return;
   const long pa = li + (long)lj * P.fni + (long)lk * P.fni * P.fnj, sz = P.siz;
-  const float *lv[3] = { P.acur, MODE == RK_MID ? P.apre : nullptr, MODE != RK_FIRST ? P.aend : nullptr };
+  const real *lv[3] = { P.acur, MODE == RK_MID ? P.apre : nullptr, MODE != RK_FIRST ? P.aend : nullptr };
 #pragma unroll
   for (int l = 0; l < 3; l++) {
     if (!lv[l]) continue;
@@ -193,14 +193,14 @@ __device__ __forceinline__ void pml_prefetch(const PmlFaceDev &P, int I, int J, 
 // with P.siz points per component)
 template <int MODE>
 __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, int d, int I, int J, int K,
-                                         const float r[9], const float D[9], const float e2[3], float lam,
-                                         float mu, float l2m, bool surf, long fidx, float corr[9]) {
+                                         const real r[9], const real D[9], const real e2[3], real lam,
+                                         real mu, real l2m, bool surf, long fidx, real corr[9]) {
   const int li = I - P.i1, lj = J - P.j1, lk = K - P.k1;
   if (li < 0 || li >= P.fni || lj < 0 || lj >= P.fnj || lk < 0 || lk >= P.fnk) return;
   const int layer = d == 0 ? li : (d == 1 ? lj : lk);
-  const float cA = __ldg(P.A + layer), cB = __ldg(P.B + layer), cD = __ldg(P.D + layer);
+  const real cA = __ldg(P.A + layer), cB = __ldg(P.B + layer), cD = __ldg(P.D + layer);
   const long pa = li + (long)lj * P.fni + (long)lk * P.fni * P.fnj;
-  float ac[9], ar[9];
+  real ac[9], ar[9];
   ld9(P.acur, P.siz, pa, ac, true);
 #pragma unroll
   for (int c = 0; c < 9; c++) {
@@ -210,11 +210,11 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
   if (surf) {
     // free-surface coupling of the x / y faces: the d-derivative of the
     // surface-converted dz velocity gradient
-    const float *X = a.free_mat + (long)(d == 0 ? 0 : 1) * a.g.ny * a.g.nx * 9 + fidx;
-    const float dd[3] = { D[VX], D[VY], D[VZ] };
-    float z[3];
+    const real *X = a.free_mat + (long)(d == 0 ? 0 : 1) * a.g.ny * a.g.nx * 9 + fidx;
+    const real dd[3] = { D[VX], D[VY], D[VZ] };
+    real z[3];
     mv3(X, dd, z);
-    float q[9];
+    real q[9];
     q[TXX] = l2m * (e2[0] * z[0]) + lam * (e2[1] * z[1] + e2[2] * z[2]);
     q[TYY] = l2m * (e2[1] * z[1]) + lam * (e2[0] * z[0] + e2[2] * z[2]);
     q[TZZ] = l2m * (e2[2] * z[2]) + lam * (e2[0] * z[0] + e2[1] * z[1]);
@@ -229,7 +229,7 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
     st9(P.aout, P.siz, pa, ac, a.ca, ar);
     st9(P.aend, P.siz, pa, ac, a.cb, ar);
   } else {
-    float pv[9], ev[9];
+    real pv[9], ev[9];
     if (MODE == RK_MID) ld9(P.apre, P.siz, pa, pv, true);
     ld9(P.aend, P.siz, pa, ev, false);
     if (MODE == RK_MID) st9(P.aout, P.siz, pa, pv, a.ca, ar);
@@ -242,13 +242,13 @@ __device__ __forceinline__ void pml_face(const VolArgs &a, const PmlFaceDev &P, 
 // and end do not alias, and interleaved load / store pairs would cost one
 // memory round trip per component.
 template <int MODE>
-__device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float v0[9], const float h[9]) {
+__device__ __forceinline__ void rk_update(const VolArgs &a, long p, const real v0[9], const real h[9]) {
   const long sc = a.g.scmp;
   if (MODE == RK_FIRST) {
     st9(a.out, sc, p, v0, a.ca, h);
     st9(a.end, sc, p, v0, a.cb, h);
   } else {
-    float pv[9], ev[9];
+    real pv[9], ev[9];
     if (MODE == RK_MID) ld9(a.pre, sc, p, pv, true);
     ld9(a.end, sc, p, ev, false);
     if (MODE == RK_MID) st9(a.out, sc, p, pv, a.ca, h);
@@ -261,7 +261,9 @@ __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const float 
 // under the free surface, with any PML faces), and the PML edges and
 // corners away from the free surface (the shell's code without the
 // free-surface logic, which keeps it in registers)
-enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4, EDGE = 5 };
+enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4, EDGE = 5, PLANE = 6 };
+// PLANE: the interior kernel's code on packed boxes: the fault planes
+// x = i0 inside the interior box, when the interior launch defers them
 
 // block -> point; boxes with a narrow x extent (PML x slabs) pack their
 // points densely instead of leaving most of a 32-wide row idle
@@ -325,17 +327,19 @@ __device__ __forceinline__ bool locate_interior(const VolArgs &a, int &i, int &j
 #endif
 
 template <int ID, int JD, int KD, int MODE, int KIND>
-__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
+__global__ void __launch_bounds__(BX * BY, KIND == INTERIOR || KIND == PLANE ? CGFD_LB_INTERIOR
                                          : (KIND == SHELL || KIND == EDGE ? CGFD_LB_SHELL : CGFD_LB_FACE))
     k_volume(const __grid_constant__ VolArgs a) {
-  static_assert(KIND >= INTERIOR && KIND <= EDGE, "kernel kind");
+  static_assert(KIND >= INTERIOR && KIND <= PLANE, "kernel kind");
   const Grid &g = a.g;
   int i, j, k;
   if (KIND == INTERIOR ? !locate_interior(a, i, j, k) : !locate(a, i, j, k)) return;
   const int I = i + NG, J = j + NG, K = k + NG;
-  // split-node slabs (i0-3..i0+3 of unwelded nodes) belong to the fault kernels
+  // split-node slabs (i0-3..i0+3 of unwelded nodes) belong to the fault
+  // kernels; with defer_i0 the fault planes go to the PLANE launch
   for (int f = 0; f < a.nfault; f++) {
     const int d = I - a.fi0[f];
+    if (KIND == INTERIOR && d == 0 && a.defer_i0) return;
     if (d >= -3 && d <= 3 && (__ldg(a.fflag[f] + J + (long)K * g.ny) & FL_SPLIT)) return;
   }
   const long p = g.at(I, J, K);
@@ -344,7 +348,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   if (MODE != RK_FIRST) {
     // the RK update reads the time-n level and the accumulator last: ask
     // L2 for their lines now, so that those reads wait on L2, not DRAM
-    const float *q[6] = { a.end + 4 * p, a.end + 4 * sc + 4 * p, a.end + 8 * sc + p,
+    const real *q[6] = { a.end + 4 * p, a.end + 4 * sc + 4 * p, a.end + 8 * sc + p,
                           a.pre + 4 * p, a.pre + 4 * sc + 4 * p, a.pre + 8 * sc + p };
 #pragma unroll
     for (int n = 0; n < (MODE == RK_MID ? 6 : 3); n++) asm volatile("prefetch.global.L2 [%0];" ::"l"(q[n]));
@@ -369,7 +373,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   }
 #endif
   // likewise the auxiliary fields of the PML faces this point lies in
-  if (KIND != INTERIOR) {
+  if (KIND != INTERIOR && KIND != PLANE) {
 #pragma unroll
     for (int f = 0; f < 6; f++) {
       if (KIND >= FACE_X && KIND <= FACE_Z && f / 2 != KIND - FACE_X) continue;
@@ -378,21 +382,21 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   }
 #endif
   const Taps w = taps_at(a.cur, sc, p);
-  float v0[9];
+  real v0[9];
   ld9(w, 0, v0);
-  const float4 r0 = coef_row(a.coef, sc, 0, p), r1 = coef_row(a.coef, sc, 1, p), r2 = coef_row(a.coef, sc, 2, p);
-  const float e[3][3] = { { r0.x, r0.y, r0.z }, { r1.x, r1.y, r1.z }, { r2.x, r2.y, r2.z } };
-  const float lam = r0.w, mu = r1.w, slw = r2.w;
-  const float l2m = lam + 2.0f * mu;
+  const real4 r0 = coef_row(a.coef, sc, 0, p), r1 = coef_row(a.coef, sc, 1, p), r2 = coef_row(a.coef, sc, 2, p);
+  const real e[3][3] = { { r0.x, r0.y, r0.z }, { r1.x, r1.y, r1.z }, { r2.x, r2.y, r2.z } };
+  const real lam = r0.w, mu = r1.w, slw = r2.w;
+  const real l2m = lam + 2.0f * mu;
   int ox[4], oy[4], oz[4];
   tap_offsets<ID>(1, ox);
   tap_offsets<JD>((int)g.sy, oy);
   tap_offsets<KD>((int)g.sz, oz);
 
-  float h[9];
-  if (KIND == INTERIOR) {
-    float G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
-    float s[3] = { 0.f, 0.f, 0.f };
+  real h[9];
+  if (KIND == INTERIOR || KIND == PLANE) {
+    real G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
+    real s[3] = { 0.f, 0.f, 0.f };
     acc_dir<ID>(w, v0, ox, e[0], G, s);
     acc_dir<JD>(w, v0, oy, e[1], G, s);
     acc_dir<KD>(w, v0, oz, e[2], G, s);
@@ -413,12 +417,12 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     // auxiliary update
     constexpr int FD = KIND - FACE_X;
     constexpr int FF = FD == 0 ? ID : (FD == 1 ? JD : KD);
-    float G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
-    float s[3] = { 0.f, 0.f, 0.f };
+    real G[3][3] = { { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f }, { 0.f, 0.f, 0.f } };
+    real s[3] = { 0.f, 0.f, 0.f };
     if (FD != 0) acc_dir<ID>(w, v0, ox, e[0], G, s);
     if (FD != 1) acc_dir<JD>(w, v0, oy, e[1], G, s);
     if (FD != 2) acc_dir<KD>(w, v0, oz, e[2], G, s);
-    float D[9], r[9], corr[9];
+    real D[9], r[9], corr[9];
     derivs<FF>(w, v0, FD == 0 ? ox : (FD == 1 ? oy : oz), D);
     rhs_dir(D, e[FD], lam, mu, l2m, slw, r);
     h[VX] = slw * s[0] + r[VX]; h[VY] = slw * s[1] + r[VY]; h[VZ] = slw * s[2] + r[VZ];
@@ -443,7 +447,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   const bool top = KIND == SHELL && a.isfree && K >= nk2 - 3;
   const bool surfrow = KIND == SHELL && a.isfree && K == nk2;
   const long fidx = ((long)J * g.nx + I) * 9;
-  float corr[9], r[9], D[9], dvx[3], dvy[3];
+  real corr[9], r[9], D[9], dvx[3], dvy[3];
 #pragma unroll
   for (int c = 0; c < 9; c++) corr[c] = 0.f;
   // x
@@ -472,22 +476,22 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
     // from the conversion matrices (surface) or from 2nd / 4th order
     // one-sided differences (one / two rows below)
     const long sz = g.sz;
-    float dz[3];
+    real dz[3];
     if (K == nk2) {
-      const float *X = a.free_mat + fidx;
-      const float *Y = X + (long)g.ny * g.nx * 9;
-      float o1[3], o2[3];
+      const real *X = a.free_mat + fidx;
+      const real *Y = X + (long)g.ny * g.nx * 9;
+      real o1[3], o2[3];
       mv3(X, dvx, o1); mv3(Y, dvy, o2);
       dz[0] = o1[0] + o2[0]; dz[1] = o1[1] + o2[1]; dz[2] = o1[2] + o2[2];
     } else if (K == nk2 - 1) {
       // velocities are components 0-2 of the first group: stride 4 floats
-      const float *v = a.cur + 4 * p;
+      const real *v = a.cur + 4 * p;
       dz[0] = mac22(v + VX, 4 * sz, KD); dz[1] = mac22(v + VY, 4 * sz, KD); dz[2] = mac22(v + VZ, 4 * sz, KD);
     } else {
-      const float *v = a.cur + 4 * p;
+      const real *v = a.cur + 4 * p;
       dz[0] = mac24(v + VX, 4 * sz, KD); dz[1] = mac24(v + VY, 4 * sz, KD); dz[2] = mac24(v + VZ, 4 * sz, KD);
     }
-    float Dz[9], rz[9];
+    real Dz[9], rz[9];
 #pragma unroll
     for (int c = 0; c < 9; c++) Dz[c] = 0.f;
     Dz[VX] = dz[0]; Dz[VY] = dz[1]; Dz[VZ] = dz[2];
@@ -502,13 +506,13 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR ? CGFD_LB_INTERIOR
   }
   if (top && K >= nk2 - (KD ? 3 : 1)) {
     // traction image on the momentum equation in the top rows
-    const float *cur = a.cur;
+    const real *cur = a.cur;
     const long sy = g.sy;
-    const float sj = slw / coef_jac(a.coef, p);
+    const real sj = slw / coef_jac(a.coef, p);
     // per tap the three traction rows at once; each row's sum over the
     // taps keeps the order of the coefficient table
-    float dx[3] = { 0.f, 0.f, 0.f }, dy[3] = { 0.f, 0.f, 0.f }, dzz[3] = { 0.f, 0.f, 0.f };
-    float t[3];
+    real dx[3] = { 0.f, 0.f, 0.f }, dy[3] = { 0.f, 0.f, 0.f }, dzz[3] = { 0.f, 0.f, 0.f };
+    real t[3];
 #pragma unroll
     for (int n = 0; n < 5; n++) {
       ctrac3(g, cur, a.coef, p + (ID ? n - 1 : n - 3), 0, t);
@@ -572,7 +576,7 @@ void launch_kind(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaS
 
 }  // namespace
 
-// This file is compiled once per kernel kind (CGFD_VOLUME_KIND = 0..5, set
+// This file is compiled once per kernel kind (CGFD_VOLUME_KIND = 0..6, set
 // by the build) so that the 24 instantiations of each kind build in
 // parallel; unit 0 also holds the host helpers.
 #ifndef CGFD_VOLUME_KIND
@@ -626,9 +630,13 @@ void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mo
 void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
   launch_kind<FACE_Z>(a, idir, jdir, kdir, mode, st);
 }
-#else
+#elif CGFD_VOLUME_KIND == 5
 void launch_volume_edge(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
   launch_kind<EDGE>(a, idir, jdir, kdir, mode, st);
+}
+#else
+void launch_volume_plane(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<PLANE>(a, idir, jdir, kdir, mode, st);
 }
 #endif
 

@@ -193,6 +193,27 @@ int cgfd_create(const cgfd_config *cfg, cgfd_solver **out);
  * Replaces the time loop of drv_rk_curv_col.cu:209-636. */
 int cgfd_run(cgfd_solver *s, int nsteps);
 
+/* Advance nsteps time steps like cgfd_run and take the fault output the
+ * reference writes while it steps: before every step whose index (steps
+ * taken so far) is a multiple of `every` (io_time_skip), the 11 fault
+ * fields of every fault, interior nodes, go to
+ * out[record][fault][11][nk][nj] (the data of io_fault_nc_put,
+ * src/forward/io_funcs.cu:2027-2099, called at drv_rk_curv_col.cu:221-226).
+ * Each record is gathered on the device into one of two staging buffers
+ * and copied on a separate stream while the next steps run; with `out` in
+ * page-locked memory the copies overlap the stepping.  `max_records`: the
+ * records `out` holds; a run that would take more is rejected with
+ * CGFD_ERR_ARG before anything runs.  *nrec: the records taken (may be
+ * NULL).  No counterpart as a function in the reference, whose loop blocks
+ * on each output copy. */
+int cgfd_run_fault_output(cgfd_solver *s, int nsteps, int every, float *out, long long max_records, int *nrec);
+
+/* Page-locked host memory for the output buffers of cgfd_run_fault_output
+ * (and any getter), for callers that do not link the CUDA runtime
+ * themselves; free it with cgfd_host_free.  No reference counterpart. */
+int cgfd_host_alloc(unsigned long long bytes, void **ptr);
+void cgfd_host_free(void *ptr);
+
 /* Number of steps taken so far. */
 int cgfd_steps_done(const cgfd_solver *s, int *it);
 
@@ -287,15 +308,22 @@ int cgfd_last_kernel_timing(const cgfd_solver *s, int which, double *ms,
  * module loading, when the library's context starts) until the process
  * exits.  Each fault needs
  * 108 * (nj_split + 6) * (nk_split + 6) floats, where nj_split x nk_split
- * is the bounding box of its split nodes.  A solver whose fault needs more
- * is rejected with CGFD_ERR_ARG before anything runs.  Faults are processed
- * one after another, so the largest one sets the need.  Nothing in the
- * array has to start at zero: every stage writes each element it reads.
+ * is the bounding box of its split nodes, rounded up to a multiple of 64.
+ * Every fault of the solver takes its own slice of the array, because the
+ * first fault kernels of a stage run for all faults before the later ones
+ * run for any of them; so the SUM over the solver's faults sets the need.
+ * A solver whose faults need more than the array holds is rejected with
+ * CGFD_ERR_ARG before anything runs.  Nothing in the array has to start at
+ * zero: every stage writes each element it reads.
  *
  * Set-up.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress).  That may also load the library's device code
- * for that device.  Make this first call before any stream capture.  Call
- * with the solver's device current, as for every entry point.
+ * (cudaGetSymbolAddress) and keeps it for later calls on that device; the
+ * address stays valid for the life of the device's primary context (a
+ * cudaDeviceReset invalidates it, so do not reset a device between calls).
+ * The look-up may also load the library's device code for that device.
+ * Make this first call before any stream capture.  Call with the solver's
+ * device current, as for every entry point.  Timing (cgfd_last_timing) is
+ * not measured here and reads 0 after this call.
  *
  * Concurrency.  The array is shared by all solvers on a device.  Calls on
  * the same device must not overlap: not from two threads, and not on two

@@ -1,0 +1,93 @@
+"""The CUDA path against the oracle at the benchmarked sizes (GPU).
+
+The benchmark runs the 600x300x240 curvilinear case (hills, layers, a
+400x180-node fault, 20-layer CFS-PML) and the 1200x600x400 case with a
+25-degree dipping fault (288 M points).  Parity is otherwise tested on
+look-alikes of a few hundred thousand points; here the block indexing, the
+y-chunked interior grid, the packed PML slabs and the 64-bit offsets run at
+the sizes they run at in the benchmark.  Each case starts from a smooth
+random wavefield plus the nucleated rupture and runs through all eight
+MacCormack operator pairs; every wavefield component and the fault fields
+are compared at relative L2 <= 1e-4.  The oracle needs host memory of the
+order of the device state (about 12 GB for 600x300x240, 80 GB for
+1200x600x400); a case is skipped, saying so, on a host with less."""
+import numpy as np
+import pytest
+
+import inputs
+from cgfd import Solver, WAVE_COMPONENTS
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _host_gb():
+    try:
+        import psutil
+        return psutil.virtual_memory().available / 2 ** 30
+    except Exception:
+        return 0.0
+
+
+def _smooth_noise(rng, shape, scale):
+    """Zero-mean noise smoothed over a few points (a wavefield the scheme
+    resolves), float32, one component at a time to bound host memory."""
+    f = rng.standard_normal(shape).astype(np.float32)
+    for ax in range(3):
+        f = 0.25 * (np.roll(f, 1, ax) + 2.0 * f + np.roll(f, -1, ax))
+    return (f * np.float32(scale / max(float(f.std()), 1e-12))).astype(np.float32)
+
+
+def _run_pair(p, nsteps, seed):
+    from oracle import OracleSolver
+    g = Solver(p)
+    o = OracleSolver(p)
+    rng = np.random.default_rng(seed)
+    for c in range(9):
+        f = _smooth_noise(rng, (p.nk, p.nj, p.ni), 1e-3 if c < 3 else 1e4)
+        g.set_wavefield(c, f)
+        o.set_wavefield(c, f)
+        del f
+    g.run(nsteps)
+    o.run(nsteps)
+    return g, o
+
+
+def _compare(g, o, p, label):
+    for c in range(9):
+        e = rel_l2(g.wavefield(c), o.wavefield(c))
+        assert e <= TOL, (label, WAVE_COMPONENTS[c], e)
+    for f in ("Vs", "Slip", "Peak_vs", "Tn", "Ts1"):
+        e = rel_l2(g.fault(f), o.fault(f))
+        assert e <= TOL, (label, f, e)
+    assert o.fault("Vs").max() > 0.01, (label, "no slip in the oracle run")
+    assert np.array_equal(g.fault("Init_t0") > 0, o.fault("Init_t0") > 0), label
+    assert rel_l2(g.stations()[:, :3], o.stations()[:, :3]) <= TOL, label
+
+
+def test_fullsize_600x300x240(cgfd_lib, oracle_built):
+    """The benchmark workload itself, 16 steps (every operator pair twice)."""
+    if _host_gb() < 40:
+        pytest.skip(f"the oracle needs about 12 GB of host memory beside the inputs; {_host_gb():.0f} GB free")
+    nt = 16
+    p = inputs.hills_layered(nt=nt)
+    g, o = _run_pair(p, nt, seed=21)
+    _compare(g, o, p, "600x300x240")
+
+
+def test_fullsize_1200x600x400(cgfd_lib, oracle_built):
+    """The 288 M-point case with the 25-degree dipping fault and von Karman
+    stress, 8 steps (every operator pair once)."""
+    if _host_gb() < 200:
+        pytest.skip(f"the oracle needs about 80 GB of host memory beside the inputs; {_host_gb():.0f} GB free")
+    nt = 8
+    p = inputs.hills_layered(ni=600, nj=1200, nk=400, h=50.0, pml=20, fault_len=800, fault_depth=360,
+                             nuc_half=30, dip=25.0, vk_stress=True, nt=nt)
+    g, o = _run_pair(p, nt, seed=22)
+    _compare(g, o, p, "1200x600x400")

@@ -270,3 +270,31 @@ def test_pool_reuse_and_release(cgfd_lib):
     assert np.array_equal(g2.wavefield("Vz"), ref)
     g2.close()
     assert cgfd_lib.cgfd_release_cached_memory() == 0
+
+
+@pytest.mark.parametrize("env", [("CGFD_BRANCHES", "0"), ("CGFD_BRANCHES", "1"), ("CGFD_BRANCHES", "3"),
+                                 ("CGFD_PRE_OVERLAP", "0")])
+def test_stage_schedules_agree(cgfd_lib, monkeypatch, env):
+    """Every stage schedule (one stream; fault, interior and PML kernels side
+    by side; the default two-stream schedule, with the stage's first fault
+    kernels beside the interior kernel and the fault planes after them, or
+    without; y / z PML slabs on a third stream) changes no arithmetic: the
+    same result bit for bit, on a case whose fault neighbourhood stays clear
+    of the PML boxes (so the next stage's fault kernels also start early)
+    and one whose fault reaches them."""
+    key, val = env
+    cases = [inputs.tpv_planar(ni=40, nj=80, nk=40, fault_x_index=21, fault_grid=[25, 56, 15, 40], nuc_half=3,
+                               pml=5, nt=20, nsta=4, margin=10),
+             inputs.small_planar(nt=20)]
+    for p in cases:
+        ref = Solver(p)
+        ref.run(17)
+        monkeypatch.setenv(key, val)
+        g = Solver(p)
+        monkeypatch.delenv(key)
+        g.run(17)
+        for f in ("Vs", "Slip", "Tn", "Ts1"):
+            assert np.array_equal(ref.fault(f), g.fault(f)), (p.name, f)
+        for c in range(9):
+            assert np.array_equal(ref.wavefield(c), g.wavefield(c)), (p.name, WAVE_COMPONENTS[c])
+        assert np.array_equal(ref.stations(), g.stations()), p.name
