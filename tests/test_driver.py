@@ -304,3 +304,28 @@ def test_driver_accepts_the_reference_par_template(cgfd_lib, tmp_path):
             "free surface 1", f"{len(p.stations)} station(s)")
     for w in want:
         assert w in r.stdout, (w, r.stdout)
+
+
+def test_reference_case_writer_keys(tmp_path):
+    """The par file the reference-pin tests give the reference's own solver
+    (tests/refcase.py) sets every top-level key its reader leaves
+    uninitialised otherwise (par_t.cu:64-900: slices, snapshots, receiver
+    lines, exports, the NaN check), keeps the welded margin at the
+    reference's fixed 40, and is accepted as it is by cgfd_run --check."""
+    import refcase
+    p = inputs.tpv_planar(ni=40, nj=100, nk=60, nt=3, pml=5, nsta=3)
+    par = refcase.write_reference_case(p, str(tmp_path / "case"), nt=3, medium="code")
+    d = json.load(open(par))
+    for k in ("receiver_line", "slice", "snapshot", "is_export_grid", "is_export_metric", "is_export_media",
+              "grid_export_dir", "media_export_dir", "check_nan_every_number_of_steps", "output_all",
+              "in_station_file", "fault_station_file", "metric_calculation_method"):
+        assert k in d, k
+    assert "welded_margin" not in d
+    assert d["slice"] == {"x_index": [], "y_index": [], "z_index": []}
+    with pytest.raises(ValueError):
+        refcase.write_reference_case(inputs.small_planar(nt=3), str(tmp_path / "c2"), nt=3)   # margin 10
+    exe = os.path.join(ROOT, "gpu-cgfd3d-dynamic_b200", "lib", "cgfd_run")
+    r = subprocess.run([exe, "--check", par], capture_output=True, text=True, timeout=120,
+                       env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+    assert r.returncode == 0, r.stderr
+    assert "4 steps" in r.stdout
