@@ -75,6 +75,14 @@ def run_reference(par_path, timeout=900):
     loop as it prints them)."""
     r = subprocess.run([REF_EXE, par_path, "0"], capture_output=True, text=True, timeout=timeout,
                        cwd=os.path.dirname(par_path))
+    with open(os.path.join(os.path.dirname(par_path), "reference.log"), "w") as fh:
+        fh.write(r.stdout + "\n---- stderr ----\n" + r.stderr)
+    logdir = os.environ.get("CGFD_REF_LOGDIR")
+    if logdir:
+        os.makedirs(logdir, exist_ok=True)
+        name = os.path.basename(os.path.dirname(par_path))
+        with open(os.path.join(logdir, f"reference_{name}.log"), "w") as fh:
+            fh.write(r.stdout[-200000:] + "\n---- stderr ----\n" + r.stderr[-50000:])
     if r.returncode != 0:
         raise RuntimeError(f"reference run failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
     m = re.search(r"Runing Time of time :\s*([0-9.eE+-]+)", r.stdout)
@@ -86,6 +94,14 @@ def read_reference_outputs(prob, par_path):
     and fault-station traces [nfsta, 9, nt_total] of a finished run."""
     par = json.load(open(par_path))
     out = par["output_dir"]
+    want = [f"fault_i{x}_px0_py0_pz0.nc" for x in prob.fault_x_index]
+    want += [f"s{q}.Vx.sac" for q in range(0 if prob.stations is None else len(prob.stations))]
+    missing = [w for w in want if not os.path.exists(os.path.join(out, w))]
+    if missing:
+        log = os.path.join(os.path.dirname(par_path), "reference.log")
+        tail = open(log).read()[-4000:] if os.path.exists(log) else ""
+        raise FileNotFoundError(f"reference outputs missing: {missing}; {out} holds {sorted(os.listdir(out))[:40]}; "
+                                f"log tail:\n{tail}")
     faults = [par_files.read_fault_output(os.path.join(out, f"fault_i{x}_px0_py0_pz0.nc"))
               for x in prob.fault_x_index]
     sta = []
