@@ -85,7 +85,7 @@ def build(verbose=False, ptxas_info=False):
     dsrc = [os.path.join(DRIVER, f) for f in DRIVER_SRC]
     dhdr = [os.path.join(DRIVER, f) for f in ("json.h", "ncclassic.h", "sac.h")] + hdrs
     if _newer(DRIVER_BIN, dsrc + dhdr + [LIB]):
-        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-o", DRIVER_BIN] + dsrc + \
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-pthread", "-o", DRIVER_BIN] + dsrc + \
               ["-L", LIBDIR, "-lcgfd", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))

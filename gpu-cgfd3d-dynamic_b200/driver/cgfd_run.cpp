@@ -31,6 +31,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cgfd.h"
@@ -420,31 +421,49 @@ int main(int argc, char **argv) {
 
   std::vector<float> fout((size_t)CGFD_FAULT_NFIELD * nk * nj);
   // the fault records of up to kChunk output steps per call, taken while
-  // the steps run into page-locked memory (cgfd_run_fault_output), then
-  // written to the files
+  // the steps run into page-locked memory (cgfd_run_fault_output); a writer
+  // thread puts one chunk's records into the files while the next chunk
+  // steps, from the other of two buffers
   const int kChunk = 32;
   const size_t rec_floats = (size_t)cfg.num_faults * CGFD_FAULT_NFIELD * nk * nj;
-  float *recs = nullptr;
-  check(cgfd_host_alloc(kChunk * rec_floats * sizeof(float), (void **)&recs), "output buffer");
-  int it = 0;
+  float *recs[2] = { nullptr, nullptr };
+  for (int b = 0; b < 2; b++)
+    check(cgfd_host_alloc(kChunk * rec_floats * sizeof(float), (void **)&recs[b]), "output buffer");
+  std::string write_error;
+  auto write_chunk = [&](const float *buf, int it0, int nrec) {
+    try {
+      for (int r = 0; r < nrec; r++) {
+        const int rit = ((it0 + skip - 1) / skip + r) * skip;   // step index of record r
+        const float tcur = (float)(rit * dt + t0);
+        for (int f = 0; f < cfg.num_faults; f++) {
+          const float *src = buf + r * rec_floats + (size_t)f * CGFD_FAULT_NFIELD * nk * nj;
+          ff[f].w->put_record_float(ff[f].vtime, rit / skip, &tcur);
+          for (int q = 0; q < 9; q++) ff[f].w->put_record_float(ff[f].vf[q], rit / skip, src + (size_t)q * nk * nj);
+        }
+      }
+    } catch (const std::exception &e) {
+      write_error = e.what();
+    }
+  };
+  std::thread writer;
+  int it = 0, chunk = 0;
   std::fprintf(stdout, "start time loop ...\n");
   const auto t_loop = std::chrono::steady_clock::now();
   while (it < nt_total) {
     const int n = std::min(kChunk * skip, nt_total - it);
     int nrec = 0;
-    check(cgfd_run_fault_output(s, n, skip, recs, kChunk, &nrec), "time steps");
-    for (int r = 0; r < nrec; r++) {
-      const int rit = ((it + skip - 1) / skip + r) * skip;   // step index of record r
-      const float tcur = (float)(rit * dt + t0);
-      for (int f = 0; f < cfg.num_faults; f++) {
-        const float *src = recs + r * rec_floats + (size_t)f * CGFD_FAULT_NFIELD * nk * nj;
-        ff[f].w->put_record_float(ff[f].vtime, rit / skip, &tcur);
-        for (int q = 0; q < 9; q++) ff[f].w->put_record_float(ff[f].vf[q], rit / skip, src + (size_t)q * nk * nj);
-      }
-    }
+    float *buf = recs[chunk & 1];          // its previous writer was joined below
+    const int rc = cgfd_run_fault_output(s, n, skip, buf, kChunk, &nrec);
+    if (writer.joinable()) writer.join();
+    check(rc, "time steps");
+    if (!write_error.empty()) die(write_error);
+    writer = std::thread(write_chunk, buf, it, nrec);
     it += n;
+    chunk++;
   }
-  cgfd_host_free(recs);
+  if (writer.joinable()) writer.join();
+  if (!write_error.empty()) die(write_error);
+  for (int b = 0; b < 2; b++) cgfd_host_free(recs[b]);
   // wall time of the time loop with its per-step fault output, the span of
   // the reference's "Runing Time" (main_curv_col_el_3d.cu:705-724)
   const double loop_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_loop).count();

@@ -89,13 +89,29 @@ def run_reference(par_path, timeout=900):
     return r.stdout + r.stderr, (float(m.group(1)) if m else float("nan"))
 
 
+def _sac_prefix(out, name):
+    """File-name prefix of a station's traces.  The reference copies each
+    station's name onto itself with sprintf (io_funcs.cu:244, :2262: source
+    and destination are the same buffer when every station lies in the
+    domain), which the C library leaves empty: every station then writes
+    ".Vx.sac" etc., and the last one's traces are what remain."""
+    return name if os.path.exists(os.path.join(out, f"{name}.Vx.sac")) or \
+        os.path.exists(os.path.join(out, f"{name}.Vs.sac")) else ""
+
+
 def read_reference_outputs(prob, par_path):
     """Fault files (one dict per fault), station traces [nsta, 9, nt_total]
-    and fault-station traces [nfsta, 9, nt_total] of a finished run."""
+    and fault-station traces [nfsta, 9, nt_total] of a finished run, with the
+    indices of the stations those traces belong to (all of them, or only the
+    last one when the reference wrote every station under an empty name)."""
     par = json.load(open(par_path))
     out = par["output_dir"]
     want = [f"fault_i{x}_px0_py0_pz0.nc" for x in prob.fault_x_index]
-    want += [f"s{q}.Vx.sac" for q in range(0 if prob.stations is None else len(prob.stations))]
+    nsta = 0 if prob.stations is None else len(prob.stations)
+    if nsta and not _sac_prefix(out, "s0"):
+        want.append(".Vx.sac")
+    elif nsta:
+        want += [f"s{q}.Vx.sac" for q in range(nsta)]
     missing = [w for w in want if not os.path.exists(os.path.join(out, w))]
     if missing:
         log = os.path.join(os.path.dirname(par_path), "reference.log")
@@ -104,10 +120,17 @@ def read_reference_outputs(prob, par_path):
                                 f"log tail:\n{tail}")
     faults = [par_files.read_fault_output(os.path.join(out, f"fault_i{x}_px0_py0_pz0.nc"))
               for x in prob.fault_x_index]
-    sta = []
-    for q in range(0 if prob.stations is None else len(prob.stations)):
-        sta.append([par_files.read_sac(os.path.join(out, f"s{q}.{c}.sac"))[3] for c in par_files.CMP])
-    fsta = []
-    for q in range(0 if prob.fault_stations is None else len(prob.fault_stations)):
-        fsta.append([par_files.read_sac(os.path.join(out, f"fault_f{q}.{c}.sac"))[3] for c in par_files.FAULT_CMP])
-    return faults, np.array(sta, np.float32), np.array(fsta, np.float32)
+    def traces(n, prefix, names, cmps):
+        if n == 0:
+            return np.zeros((0, len(cmps), 0), np.float32), []
+        if _sac_prefix(out, prefix + names[0]):
+            idx = list(range(n))
+            tr = [[par_files.read_sac(os.path.join(out, f"{prefix}{names[q]}.{c}.sac"))[3] for c in cmps] for q in idx]
+        else:
+            idx = [n - 1]
+            tr = [[par_files.read_sac(os.path.join(out, f"{prefix}.{c}.sac"))[3] for c in cmps]]
+        return np.array(tr, np.float32), idx
+    sta, sta_idx = traces(nsta, "", [f"s{q}" for q in range(nsta)], par_files.CMP)
+    nf = 0 if prob.fault_stations is None else len(prob.fault_stations)
+    fsta, fsta_idx = traces(nf, "fault_", [f"f{q}" for q in range(nf)], par_files.FAULT_CMP)
+    return faults, sta, fsta, sta_idx, fsta_idx
