@@ -133,7 +133,12 @@ def _check_solver(solver, R, every, label):
         for c, name in enumerate(par_files.FAULT_CMP):
             if name in ("Ts2", "Vs2", "Slip2"):
                 continue
-            assert rel_l2(fs[:, c], R["fsta"][:, c]) <= TOL, (label, "fault station", name)
+            mine, ref = fs[:, c], R["fsta"][:, c]
+            if name in ("Vs", "Vs1", "Slip", "Slip1") and np.abs(ref).max() < 1e-6 and np.abs(mine).max() < 1e-6:
+                # a node the rupture has not reached: slip rate and slip are
+                # rounding noise of a zero velocity jump in both runs
+                continue
+            assert rel_l2(mine, ref) <= TOL, (label, "fault station", name)
     if R["pg"] is not None:
         from cgfd import PEAK_FIELDS
         mine = solver.surface_peaks()
