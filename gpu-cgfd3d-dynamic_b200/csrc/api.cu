@@ -864,7 +864,16 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
   {
     const char *br = std::getenv("CGFD_BRANCHES");
     if (br) s->branches = std::atoi(br);
-    for (int q = 0; q < 3; q++) CK(cudaStreamCreateWithFlags(&s->aux[q], cudaStreamNonBlocking), "stream");
+    // the fault stream at the device's highest priority: the fault kernels
+    // run beside whole-grid volume kernels, and their blocks should take
+    // free SM slots first rather than wait for the volume grid's last wave
+    // (CGFD_FAULT_PRIORITY=0: default priority)
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "stream priorities");
+    const char *fp = std::getenv("CGFD_FAULT_PRIORITY");
+    const bool hi = !(fp && fp[0] == '0');
+    for (int q = 0; q < 3; q++)
+      CK(cudaStreamCreateWithPriority(&s->aux[q], cudaStreamNonBlocking, q == 0 && hi ? prio_hi : prio_lo), "stream");
     for (int a = 0; a < 4; a++) {
       CK(cudaEventCreateWithFlags(&s->ev_stage[a], cudaEventDisableTiming), "event");
       CK(cudaEventCreateWithFlags(&s->ev_predone[a], cudaEventDisableTiming), "event");
