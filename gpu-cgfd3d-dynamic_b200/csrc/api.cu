@@ -103,9 +103,10 @@ struct cgfd_solver {
   cudaEvent_t ev_int0[8][4] = {};       // before it
   // concurrent branches of a stage: 0 none; 1 fault slabs and nodes, PML
   // slabs and shell beside the interior kernel; 2 the interior kernel
-  // alone, then the fault slabs and nodes beside the PML slabs and shell
-  // (CGFD_BRANCHES): streams and fork / join events
-  int branches = 2;
+  // alone, then the fault slabs and nodes beside the PML slabs and shell;
+  // 3 as 2 with the y and z PML slabs on a third stream from the interior
+  // kernel's issue on (CGFD_BRANCHES): streams and fork / join events
+  int branches = 3;
   cudaStream_t aux[3] = {};
   cudaEvent_t ev_fork[4] = {}, ev_join[4][3] = {}, ev_pre[4] = {};
   // the next stage's first fault kernels may overlap this stage's PML slab
@@ -114,6 +115,11 @@ struct cgfd_solver {
   // the interior kernel defers the fault planes x = i0 to a PLANE launch
   // and so runs beside the stage's first fault kernels (CGFD_PRE_OVERLAP)
   bool pre_overlap = false;
+  // with pre_overlap: the fault slab kernels follow the stage's first fault
+  // kernels on the fault stream at once, beside the interior kernel (and,
+  // for stages 2-4, the previous stage's PML kernels), instead of after the
+  // interior kernel (CGFD_POST_EARLY)
+  bool post_early = true;
   cudaEvent_t ev_stage[4] = {}, ev_predone[4] = {}, ev_postdone[4] = {};
   double run_ms = 0, vol_ms = 0, int_ms = 0;
   long long vol_launches = 0, int_launches = 0;
@@ -320,9 +326,14 @@ void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = tru
   // branches 3: as 2, and the y and z PML slab kernels run on a third
   // stream beside the x slab, edge and surface-row kernels (disjoint
   // points, the same input), so that their launch gaps and tails overlap
+  // (the default).  With post_early the fault slab kernels follow the first
+  // fault kernels on the fault stream at once: the slab points' input is
+  // complete then, and the lines of the fault neighbourhood that the first
+  // kernels brought into L2 are still there
   const bool br = s->branches == 1, br2 = s->branches >= 2, br3 = s->branches == 3;
   const bool early = br2 && s->pre_early;
   const bool ov = br2 && s->pre_overlap;
+  const bool pe2 = ov && s->post_early;
   FaultArgs fargs[MAXF], fnext[MAXF];
   const int nfa = stage_fargs(0, fargs);
   for (int stage = 0; stage < 4; stage++) {
@@ -344,11 +355,15 @@ void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = tru
         cudaEventRecord(s->ev_stage[stage], s->stream);
         cudaStreamWaitEvent(s->aux[0], s->ev_stage[stage], 0);
         for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fargs[f], s->aux[0]);
+        cudaEventRecord(s->ev_predone[stage], s->aux[0]);
+        if (pe2) {
+          for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], s->aux[0]);
+          cudaEventRecord(s->ev_postdone[stage], s->aux[0]);
+        }
       } else {
         for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fargs[f], s->stream);
       }
     }
-    if (ov) cudaEventRecord(s->ev_predone[stage], s->aux[0]);
     // external event nodes when captured, so that the events really fire
     // on every graph replay; the stage interval spans the fork to the join
     if (tm) cudaEventRecordWithFlags(s->ev_vol[ip][stage][0], s->stream, cudaEventRecordExternal);
@@ -393,10 +408,12 @@ void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = tru
           // now overlap the PML slabs and the shell
           st_fault = s->aux[0];
           cudaEventRecord(s->ev_fork[stage], s->stream);
-          cudaStreamWaitEvent(st_fault, s->ev_fork[stage], 0);
           if (br3) cudaStreamWaitEvent(s->aux[1], s->ev_fork[stage], 0);
-          for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
-          if (ov) cudaEventRecord(s->ev_postdone[stage], st_fault);
+          if (!pe2) {
+            cudaStreamWaitEvent(st_fault, s->ev_fork[stage], 0);
+            for (int f = 0; f < nfa; f++) nl += launch_fault_post(fargs[f], st_fault);
+            if (ov) cudaEventRecord(s->ev_postdone[stage], st_fault);
+          }
         }
         if (kind == 2 && early && stage < 3) {
           // the surface rows are issued: the next stage's input is complete
@@ -405,6 +422,15 @@ void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = tru
           cudaStreamWaitEvent(st_fault, s->ev_pre[stage], 0);
           stage_fargs(stage + 1, fnext);
           for (int f = 0; f < nfa; f++) nl += launch_fault_pre(fnext[f], st_fault);
+          if (ov) cudaEventRecord(s->ev_predone[stage + 1], st_fault);
+          if (pe2) {
+            // the slab points' input is complete as well (the PML boxes
+            // and their stencils stay clear of the fault neighbourhood), and
+            // no kernel of this stage reads or writes the next stage's
+            // output or end level there
+            for (int f = 0; f < nfa; f++) nl += launch_fault_post(fnext[f], st_fault);
+            cudaEventRecord(s->ev_postdone[stage + 1], st_fault);
+          }
         }
         VolArgs vk = vs;
         volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind != 0 && s->pack);
@@ -812,6 +838,8 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     s->pre_overlap = !s->faults.empty();
     const char *po = std::getenv("CGFD_PRE_OVERLAP");
     if (po && po[0] == '0') s->pre_overlap = false;
+    const char *pq = std::getenv("CGFD_POST_EARLY");
+    if (pq && pq[0] == '0') s->post_early = false;
     const char *pk = std::getenv("CGFD_PACK");
     if (pk && pk[0] == '0') s->pack = false;
     // y tiles (8 rows) per interior chunk: the z window of a chunk, about 8

@@ -65,6 +65,18 @@ __device__ __forceinline__ void trac3(const Grid &g, const real *__restrict__ w,
   t[2] = J * (ex * sxz + ey * syz + ez * szz);
 }
 
+// odd extension of a 7-point line about its entry nf (3..6, the free
+// surface): v[nf] = 0 and v[nf + l] = -v[nf - l] beyond it.  Fixed indices
+// in every case keep the line in registers.
+__device__ __forceinline__ void odd_image(real v[7], int nf) {
+  switch (nf) {
+    case 3: v[3] = 0.f; v[4] = -v[2]; v[5] = -v[1]; v[6] = -v[0]; break;
+    case 4: v[4] = 0.f; v[5] = -v[3]; v[6] = -v[2]; break;
+    case 5: v[5] = 0.f; v[6] = -v[4]; break;
+    default: v[6] = 0.f; break;
+  }
+}
+
 // stage update of N values; every level read is issued before the first
 // store (the compiler cannot prove that the levels do not alias, and
 // interleaved load / store pairs cost one memory round trip each)
@@ -238,8 +250,7 @@ __device__ __forceinline__ void split_trial(const FaultArgs &a, int j, int k, ui
         real v[7];
 #pragma unroll
         for (int l = 0; l < 7; l++) v[l] = __ldg(t3 + (long)(l - 3) * ny);
-        v[nf] = 0.f;
-        for (int l = nf + 1; l < 7; l++) v[l] = -v[2 * nf - l];
+        odd_image(v, nf);
         dz = drp_v(v + 3, a.kdir);
       } else {
         dz = (fl & FL_RUPZ) ? mac22(t3, ny, a.kdir) : drp_rt(t3, ny, a.kdir);
@@ -402,8 +413,7 @@ __device__ __forceinline__ void slab_velocity(const FaultArgs &a, int j, int k, 
       z[l] = t3[c * pl + (l - 3) * row];
     }
     if (surf) {
-      z[nf] = 0.f;
-      for (int l = nf + 1; l < 7; l++) z[l] = -z[2 * nf - l];
+      odd_image(z, nf);
     }
     hv3[c] = (hv[c] + drp_v(y + 3, a.jdir) + drp_v(z + 3, a.kdir)) * rr;
   }

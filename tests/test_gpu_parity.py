@@ -272,13 +272,15 @@ def test_pool_reuse_and_release(cgfd_lib):
     assert cgfd_lib.cgfd_release_cached_memory() == 0
 
 
-@pytest.mark.parametrize("env", [("CGFD_BRANCHES", "0"), ("CGFD_BRANCHES", "1"), ("CGFD_BRANCHES", "3"),
-                                 ("CGFD_PRE_OVERLAP", "0")])
+@pytest.mark.parametrize("env", [("CGFD_BRANCHES", "0"), ("CGFD_BRANCHES", "1"), ("CGFD_BRANCHES", "2"),
+                                 ("CGFD_PRE_OVERLAP", "0"), ("CGFD_POST_EARLY", "0")])
 def test_stage_schedules_agree(cgfd_lib, monkeypatch, env):
     """Every stage schedule (one stream; fault, interior and PML kernels side
-    by side; the default two-stream schedule, with the stage's first fault
-    kernels beside the interior kernel and the fault planes after them, or
-    without; y / z PML slabs on a third stream) changes no arithmetic: the
+    by side; the interior kernel alone, then the fault slabs beside the PML
+    kernels; the default, with the y / z PML slabs on a third stream, the
+    stage's first fault kernels beside the interior kernel and the fault
+    planes after them, and the fault slabs right after the first fault
+    kernels; each of those last two switched off) changes no arithmetic: the
     same result bit for bit, on a case whose fault neighbourhood stays clear
     of the PML boxes (so the next stage's fault kernels also start early)
     and one whose fault reaches them."""
