@@ -419,6 +419,39 @@ __device__ __forceinline__ void slab_velocity(const FaultArgs &a, int j, int k, 
   }
 }
 
+// component c (0 x, 1 y, 2 z) of a 16-byte group
+__device__ __forceinline__ real cmp3(const real4 &v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+// drp, mac24 and mac22 (same weights, same order of the sums) of the three
+// velocity components along stride st (in groups) from whole 16-byte groups
+// (Vx Vy Vz Txx) of one level, direction f
+__device__ __forceinline__ void vel_drp(const real4 *__restrict__ p, long st, int f, real o[3]) {
+  if (f) {
+    const real4 a = __ldg(p - st), b = __ldg(p), c = __ldg(p + st), d = __ldg(p + 2 * st), e = __ldg(p + 3 * st);
+#pragma unroll
+    for (int n = 0; n < 3; n++)
+      o[n] = kC1 * cmp3(a, n) + kC2 * cmp3(b, n) + kC3 * cmp3(c, n) + kC4 * cmp3(d, n) + kC5 * cmp3(e, n);
+  } else {
+    const real4 a = __ldg(p + st), b = __ldg(p), c = __ldg(p - st), d = __ldg(p - 2 * st), e = __ldg(p - 3 * st);
+#pragma unroll
+    for (int n = 0; n < 3; n++)
+      o[n] = -(kC1 * cmp3(a, n) + kC2 * cmp3(b, n) + kC3 * cmp3(c, n) + kC4 * cmp3(d, n) + kC5 * cmp3(e, n));
+  }
+}
+__device__ __forceinline__ void vel_mac24(const real4 *__restrict__ p, long st, int f, real o[3]) {
+  const real4 b = __ldg(p), c = __ldg(f ? p + st : p - st), d = __ldg(f ? p + 2 * st : p - 2 * st);
+#pragma unroll
+  for (int n = 0; n < 3; n++) {
+    const real t = kB1 * cmp3(b, n) + kB2 * cmp3(c, n) + kB3 * cmp3(d, n);
+    o[n] = f ? t : -t;
+  }
+}
+__device__ __forceinline__ void vel_mac22(const real4 *__restrict__ p, long st, int f, real o[3]) {
+  const real4 b = __ldg(p), c = __ldg(f ? p + st : p - st);
+#pragma unroll
+  for (int n = 0; n < 3; n++) o[n] = f ? cmp3(c, n) - cmp3(b, n) : cmp3(b, n) - cmp3(c, n);
+}
+
 // ---------------------------------------------------------------------------
 // stress RHS and RK update at the six volume points i0-3..i0+3 (not i0) of
 // split nodes, one thread per point, x offset fastest
@@ -430,8 +463,6 @@ __device__ __forceinline__ void slab_stress(const FaultArgs &a, int j, int k, in
   const long ns = (long)g.ny * g.nz, nd = J + (long)K * g.ny, sc = g.scmp;
   const int i0 = a.F.i0;
   const real *w = a.wcur;
-  // velocity components sit 4 floats apart from one point to the next
-  const long sy = 4 * g.sy, sz = 4 * g.sz;
   const int km = g.nk - (k + 1);
   const bool fwd = a.idir == 1;
   const bool top = a.isfree && km == 0;
@@ -441,32 +472,51 @@ __device__ __forceinline__ void slab_stress(const FaultArgs &a, int j, int k, in
 #pragma unroll
   for (int c = 0; c < 3; c++) fV[c] = a.fc[fidx(FVX + c, m, ns, nd)];
   const long q = g.at(i0 + s, J, K);
+  // the velocity taps as whole 16-byte groups (Vx Vy Vz Txx): one load per
+  // tap for all three components
+  const real4 *V = reinterpret_cast<const real4 *>(w) + q;
+  const real4 v0 = __ldg(V);
   real dx[3], dy[3], dz[3];
+  if (fwd) {
+    // forward operators; points left of the fault see the minus side
+    if (s == 3) vel_drp(V, 1, 1, dx);
+    else if (s == 2) vel_mac24(V, 1, 1, dx);
+    else if (s == 1) vel_mac22(V, 1, 1, dx);
+    else if (s == -1) {
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    const real *v = w + g.w(VX + c, q);
-    const real f = fV[c];
-    if (fwd) {
-      // forward operators; points left of the fault see the minus side
-      if (s == 3) dx[c] = drp<1>(v, 4);
-      else if (s == 2) dx[c] = mac24(v, 4, 1);
-      else if (s == 1) dx[c] = mac22(v, 4, 1);
-      else if (s == -1) dx[c] = f - __ldg(v);
-      else if (s == -2) dx[c] = kB1 * __ldg(v) + kB2 * __ldg(v + 4) + kB3 * f;
-      else dx[c] = kC1 * __ldg(v - 4) + kC2 * __ldg(v) + kC3 * __ldg(v + 4) + kC4 * __ldg(v + 8) + kC5 * f;
+      for (int c = 0; c < 3; c++) dx[c] = fV[c] - cmp3(v0, c);
+    } else if (s == -2) {
+      const real4 v1 = __ldg(V + 1);
+#pragma unroll
+      for (int c = 0; c < 3; c++) dx[c] = kB1 * cmp3(v0, c) + kB2 * cmp3(v1, c) + kB3 * fV[c];
     } else {
-      if (s == -3) dx[c] = drp<0>(v, 4);
-      else if (s == -2) dx[c] = mac24(v, 4, 0);
-      else if (s == -1) dx[c] = mac22(v, 4, 0);
-      else if (s == 1) dx[c] = __ldg(v) - f;
-      else if (s == 2) dx[c] = -(kB3 * f + kB2 * __ldg(v - 4) + kB1 * __ldg(v));
-      else dx[c] = -(kC5 * f + kC4 * __ldg(v - 8) + kC3 * __ldg(v - 4) + kC2 * __ldg(v) + kC1 * __ldg(v + 4));
+      const real4 vm = __ldg(V - 1), v1 = __ldg(V + 1), v2 = __ldg(V + 2);
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        dx[c] = kC1 * cmp3(vm, c) + kC2 * cmp3(v0, c) + kC3 * cmp3(v1, c) + kC4 * cmp3(v2, c) + kC5 * fV[c];
     }
-    dy[c] = drp_rt(v, sy, a.jdir);
-    if (a.isfree && km == 1) dz[c] = mac22(v, sz, a.kdir);
-    else if (a.isfree && km == 2) dz[c] = mac24(v, sz, a.kdir);
-    else dz[c] = drp_rt(v, sz, a.kdir);
+  } else {
+    if (s == -3) vel_drp(V, 1, 0, dx);
+    else if (s == -2) vel_mac24(V, 1, 0, dx);
+    else if (s == -1) vel_mac22(V, 1, 0, dx);
+    else if (s == 1) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) dx[c] = cmp3(v0, c) - fV[c];
+    } else if (s == 2) {
+      const real4 vm = __ldg(V - 1);
+#pragma unroll
+      for (int c = 0; c < 3; c++) dx[c] = -(kB3 * fV[c] + kB2 * cmp3(vm, c) + kB1 * cmp3(v0, c));
+    } else {
+      const real4 vm2 = __ldg(V - 2), vm = __ldg(V - 1), v1 = __ldg(V + 1);
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        dx[c] = -(kC5 * fV[c] + kC4 * cmp3(vm2, c) + kC3 * cmp3(vm, c) + kC2 * cmp3(v0, c) + kC1 * cmp3(v1, c));
+    }
   }
+  vel_drp(V, g.sy, a.jdir, dy);
+  if (a.isfree && km == 1) vel_mac22(V, g.sz, a.kdir, dz);
+  else if (a.isfree && km == 2) vel_mac24(V, g.sz, a.kdir, dz);
+  else vel_drp(V, g.sz, a.kdir, dz);
   if (top) {
     const real *X = a.free_mat + ((long)J * g.nx + (i0 + s)) * 9;
     const real *Y = X + (long)g.ny * g.nx * 9;
