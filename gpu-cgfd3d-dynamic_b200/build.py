@@ -22,7 +22,7 @@ NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 
 # (source, object, extra flags): the volume kernels build as one unit per
 # kernel kind so that they compile in parallel
-CU = [("volume.cu", f"volume_k{k}.cu.o", [f"-DCGFD_VOLUME_KIND={k}"]) for k in range(7)] + [
+CU = [("volume.cu", f"volume_k{k}.cu.o", [f"-DCGFD_VOLUME_KIND={k}"]) for k in range(8)] + [
     (f, f + ".o", []) for f in ("fault.cu", "boundary.cu", "noalloc.cu", "api.cu")]
 CPP = ["setup.cpp"]
 DRIVER = os.path.join(HERE, "driver")

@@ -33,6 +33,7 @@ void launch_volume_face_y(const VolArgs &a, int idir, int jdir, int kdir, int mo
 void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_edge(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 void launch_volume_plane(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
+void launch_volume_top(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st);
 int launch_fault_pre(const FaultArgs &a, cudaStream_t st);
 int launch_fault_post(const FaultArgs &a, cudaStream_t st);
 cudaError_t noalloc_scratch_address(real **p);
@@ -131,8 +132,8 @@ struct cgfd_solver {
   // boxes of each volume kernel kind: 0 interior, 1 generic shell (PML
   // edges / corners, surface rows), 2..4 slabs reached by the PML faces of
   // one direction only (x, y, z)
-  int kbox[7][12][6];
-  int nkbox[7] = {};
+  int kbox[8][12][6];
+  int nkbox[8] = {};
   std::vector<void *> allocs;
   // cgfd_run_fault_output: two device staging buffers of one record (all
   // faults' 11 fields at interior nodes), a copy stream and the events that
@@ -431,6 +432,13 @@ void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = tru
             for (int f = 0; f < nfa; f++) nl += launch_fault_post(fnext[f], st_fault);
             cudaEventRecord(s->ev_postdone[stage + 1], st_fault);
           }
+        }
+        if (kind == 1) {
+          // surface rows away from every PML face, beside (before) the
+          // shell's rows in the PML columns
+          VolArgs vt = vs;
+          volume_boxes(vt, s->kbox[7], s->nkbox[7], s->pack);
+          if (vt.nbox > 0) { launch_volume_top(vt, idir, jdir, kdir, mode, st_pml); nl++; }
         }
         VolArgs vk = vs;
         volume_boxes(vk, s->kbox[kind], s->nkbox[kind], kind != 0 && s->pack);
@@ -804,7 +812,15 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     add(5, ihi + 1, ni - 1, 0, nj - 1, 0, klo - 1);
     add(5, ilo, ihi, 0, jlo - 1, 0, klo - 1);
     add(5, ilo, ihi, jhi + 1, nj - 1, 0, klo - 1);
-    if (s->isfree) {
+    const char *tp = std::getenv("CGFD_TOP");
+    if (s->isfree && khi + 1 >= klo && !(tp && tp[0] == '0')) {
+      // the rows of the PML columns (shell) and the rest (top kernel)
+      add(7, ilo, ihi, jlo, jhi, khi + 1, nk - 1);
+      add(1, 0, ilo - 1, 0, nj - 1, khi + 1, nk - 1);
+      add(1, ihi + 1, ni - 1, 0, nj - 1, khi + 1, nk - 1);
+      add(1, ilo, ihi, 0, jlo - 1, khi + 1, nk - 1);
+      add(1, ilo, ihi, jhi + 1, nj - 1, khi + 1, nk - 1);
+    } else if (s->isfree) {
       add(1, 0, ni - 1, 0, nj - 1, khi + 1, nk - 1);
     } else {
       add(5, 0, ilo - 1, 0, nj - 1, khi + 1, nk - 1);

@@ -261,9 +261,11 @@ __device__ __forceinline__ void rk_update(const VolArgs &a, long p, const real v
 // under the free surface, with any PML faces), and the PML edges and
 // corners away from the free surface (the shell's code without the
 // free-surface logic, which keeps it in registers)
-enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4, EDGE = 5, PLANE = 6 };
+enum { INTERIOR = 0, SHELL = 1, FACE_X = 2, FACE_Y = 3, FACE_Z = 4, EDGE = 5, PLANE = 6, TOP = 7 };
 // PLANE: the interior kernel's code on packed boxes: the fault planes
-// x = i0 inside the interior box, when the interior launch defers them
+// x = i0 inside the interior box, when the interior launch defers them.
+// TOP: the shell's code without the PML faces, for the rows under the free
+// surface away from every PML face (fewer live values than the shell)
 
 // block -> point; boxes with a narrow x extent (PML x slabs) pack their
 // points densely instead of leaving most of a 32-wide row idle
@@ -319,6 +321,9 @@ __device__ __forceinline__ bool locate_interior(const VolArgs &a, int &i, int &j
 #ifndef CGFD_LB_INTERIOR
 #define CGFD_LB_INTERIOR 4
 #endif
+#ifndef CGFD_LB_TOP
+#define CGFD_LB_TOP 3
+#endif
 #ifndef CGFD_LB_SHELL
 #define CGFD_LB_SHELL 3
 #endif
@@ -328,9 +333,10 @@ __device__ __forceinline__ bool locate_interior(const VolArgs &a, int &i, int &j
 
 template <int ID, int JD, int KD, int MODE, int KIND>
 __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR || KIND == PLANE ? CGFD_LB_INTERIOR
-                                         : (KIND == SHELL || KIND == EDGE ? CGFD_LB_SHELL : CGFD_LB_FACE))
+                                         : (KIND == SHELL || KIND == EDGE ? CGFD_LB_SHELL
+                                                                          : (KIND == TOP ? CGFD_LB_TOP : CGFD_LB_FACE)))
     k_volume(const __grid_constant__ VolArgs a) {
-  static_assert(KIND >= INTERIOR && KIND <= PLANE, "kernel kind");
+  static_assert(KIND >= INTERIOR && KIND <= TOP, "kernel kind");
   const Grid &g = a.g;
   int i, j, k;
   if (KIND == INTERIOR ? !locate_interior(a, i, j, k) : !locate(a, i, j, k)) return;
@@ -373,7 +379,7 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR || KIND == PLANE ? C
   }
 #endif
   // likewise the auxiliary fields of the PML faces this point lies in
-  if (KIND != INTERIOR && KIND != PLANE) {
+  if (KIND != INTERIOR && KIND != PLANE && KIND != TOP) {
 #pragma unroll
     for (int f = 0; f < 6; f++) {
       if (KIND >= FACE_X && KIND <= FACE_Z && f / 2 != KIND - FACE_X) continue;
@@ -444,8 +450,9 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR || KIND == PLANE ? C
 
   // ---- shell and edges: PML edges and corners, rows under the free surface
   const int nk2 = g.nk + NG - 1;
-  const bool top = KIND == SHELL && a.isfree && K >= nk2 - 3;
-  const bool surfrow = KIND == SHELL && a.isfree && K == nk2;
+  const bool top = (KIND == SHELL || KIND == TOP) && a.isfree && K >= nk2 - 3;
+  const bool surfrow = (KIND == SHELL || KIND == TOP) && a.isfree && K == nk2;
+  constexpr bool pml = KIND != TOP;
   const long fidx = ((long)J * g.nx + I) * 9;
   real corr[9], r[9], D[9], dvx[3], dvy[3];
 #pragma unroll
@@ -456,21 +463,21 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR || KIND == PLANE ? C
   rhs_dir(D, e[0], lam, mu, l2m, slw, r);
 #pragma unroll
   for (int c = 0; c < 9; c++) h[c] = r[c];
-  if (a.pml[0].on) pml_face<MODE>(a, a.pml[0], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
-  if (a.pml[1].on) pml_face<MODE>(a, a.pml[1], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  if (pml && a.pml[0].on) pml_face<MODE>(a, a.pml[0], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  if (pml && a.pml[1].on) pml_face<MODE>(a, a.pml[1], 0, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
   // y
   derivs<JD>(w, v0, oy, D);
   dvy[0] = D[VX]; dvy[1] = D[VY]; dvy[2] = D[VZ];
   rhs_dir(D, e[1], lam, mu, l2m, slw, r);
 #pragma unroll
   for (int c = 0; c < 9; c++) h[c] += r[c];
-  if (a.pml[2].on) pml_face<MODE>(a, a.pml[2], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
-  if (a.pml[3].on) pml_face<MODE>(a, a.pml[3], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  if (pml && a.pml[2].on) pml_face<MODE>(a, a.pml[2], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
+  if (pml && a.pml[3].on) pml_face<MODE>(a, a.pml[3], 1, I, J, K, r, D, e[2], lam, mu, l2m, surfrow, fidx, corr);
   // z
   derivs<KD>(w, v0, oz, D);
   rhs_dir(D, e[2], lam, mu, l2m, slw, r);
-  if (a.pml[4].on) pml_face<MODE>(a, a.pml[4], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
-  if (a.pml[5].on) pml_face<MODE>(a, a.pml[5], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
+  if (pml && a.pml[4].on) pml_face<MODE>(a, a.pml[4], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
+  if (pml && a.pml[5].on) pml_face<MODE>(a, a.pml[5], 2, I, J, K, r, D, e[2], lam, mu, l2m, false, fidx, corr);
   if (top && K >= nk2 - 2) {
     // velocity below the surface: the z part of the velocity gradient comes
     // from the conversion matrices (surface) or from 2nd / 4th order
@@ -576,7 +583,7 @@ void launch_kind(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaS
 
 }  // namespace
 
-// This file is compiled once per kernel kind (CGFD_VOLUME_KIND = 0..6, set
+// This file is compiled once per kernel kind (CGFD_VOLUME_KIND = 0..7, set
 // by the build) so that the 24 instantiations of each kind build in
 // parallel; unit 0 also holds the host helpers.
 #ifndef CGFD_VOLUME_KIND
@@ -634,9 +641,13 @@ void launch_volume_face_z(const VolArgs &a, int idir, int jdir, int kdir, int mo
 void launch_volume_edge(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
   launch_kind<EDGE>(a, idir, jdir, kdir, mode, st);
 }
-#else
+#elif CGFD_VOLUME_KIND == 6
 void launch_volume_plane(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
   launch_kind<PLANE>(a, idir, jdir, kdir, mode, st);
+}
+#else
+void launch_volume_top(const VolArgs &a, int idir, int jdir, int kdir, int mode, cudaStream_t st) {
+  launch_kind<TOP>(a, idir, jdir, kdir, mode, st);
 }
 #endif
 

@@ -300,3 +300,31 @@ def test_stage_schedules_agree(cgfd_lib, monkeypatch, env):
         for c in range(9):
             assert np.array_equal(ref.wavefield(c), g.wavefield(c)), (p.name, WAVE_COMPONENTS[c])
         assert np.array_equal(ref.stations(), g.stations()), p.name
+
+
+def test_surface_rows_kernels_agree(cgfd_lib, monkeypatch):
+    """The rows under the free surface away from the PML columns run in a
+    kernel of their own, the shell's code without the PML faces; with it
+    switched off (CGFD_TOP=0) the shell kernel updates all surface rows.
+    Without the PML terms the compiler fuses some multiply-adds of the
+    direction sums differently, so the two agree to rounding (relative L2
+    <= 1e-6 after 17 steps, measured ~3e-8), not bit for bit."""
+    cases = [inputs.tpv_planar(ni=40, nj=80, nk=40, fault_x_index=21, fault_grid=[25, 56, 15, 40], nuc_half=3,
+                               pml=5, nt=20, nsta=4, margin=10),
+             inputs.small_planar(nt=20, dynamic_method=2)]
+    for p in cases:
+        ref = Solver(p)
+        ref.run(17)
+        monkeypatch.setenv("CGFD_TOP", "0")
+        g = Solver(p)
+        monkeypatch.delenv("CGFD_TOP")
+        g.run(17)
+        if p is cases[0]:
+            # PML columns on every side: one launch more per stage with the
+            # surface rows split
+            assert ref.last_launches() == g.last_launches() + 4 * 17, (ref.last_launches(), g.last_launches())
+        for f in ("Vs", "Slip", "Tn", "Ts1"):
+            assert rel_l2(ref.fault(f), g.fault(f)) <= 1e-6, (p.name, f)
+        for c in range(9):
+            assert rel_l2(ref.wavefield(c), g.wavefield(c)) <= 1e-6, (p.name, WAVE_COMPONENTS[c])
+        assert rel_l2(ref.stations(), g.stations()) <= 1e-6, p.name
