@@ -273,6 +273,22 @@ size_t trac_slices(const cgfd_solver *s, size_t *off) {
 // split into one slice per fault because the first fault kernels of every
 // fault run before the later ones of any fault; timed: whether the
 // solver's timing events may be recorded
+// the fault planes of a volume launch: x = i0 of each fault, its split-node
+// flags and the deferred box (the split box grown by 3 nodes, empty when the
+// fault has no split node)
+void fault_planes(const cgfd_solver *s, VolArgs &v) {
+  for (size_t f = 0; f < s->faults.size(); f++) {
+    const FaultState &F = s->faults[f];
+    v.fi0[f] = F.d.i0;
+    v.fflag[f] = F.flag;
+    const bool any = F.nj > 0 && F.nk > 0;
+    v.fdef[f][0] = any ? F.j0 - 3 + NG : 1;
+    v.fdef[f][1] = any ? F.j0 + F.nj + 2 + NG : 0;
+    v.fdef[f][2] = any ? F.k0 - 3 + NG : 1;
+    v.fdef[f][3] = any ? F.k0 + F.nk + 2 + NG : 0;
+  }
+}
+
 void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = true) {
   const int ip = it % 8;
   const bool tm = s->timing && timed;
@@ -384,7 +400,7 @@ void enqueue_step(cgfd_solver *s, int it, real *trac = nullptr, bool timed = tru
     v.ca = ca; v.cb = cb; v.isfree = s->isfree;
     v.nfault = (int)s->faults.size();
     v.defer_i0 = ov ? 1 : 0;
-    for (size_t f = 0; f < s->faults.size(); f++) { v.fi0[f] = s->faults[f].d.i0; v.fflag[f] = s->faults[f].flag; }
+    fault_planes(s, v);
     for (int q = 0; q < 6; q++) {
       v.pml[q] = s->pml[q].d;
       if (!v.pml[q].on) continue;
@@ -615,6 +631,7 @@ int cgfd_create(const cgfd_config *cfg, cgfd_solver **out) {
 
 static int build_graphs(cgfd_solver *s);
 
+
 // Autotuner of the interior kernel's y chunk (the number of 8-row tiles whose
 // blocks march up z together, which sets how much of L2 the stencil planes
 // take): the first stage's interior launch is timed for a few chunk sizes
@@ -642,7 +659,7 @@ static cudaError_t tune_ychunk(cgfd_solver *s) {
   v.coef = s->coef; v.free_mat = s->free_mat;
   v.ca = kRkA[0] * s->dt; v.cb = kRkB[0] * s->dt; v.isfree = s->isfree;
   v.nfault = (int)s->faults.size();
-  for (size_t f = 0; f < s->faults.size(); f++) { v.fi0[f] = s->faults[f].d.i0; v.fflag[f] = s->faults[f].flag; }
+  fault_planes(s, v);
   volume_boxes(v, s->kbox[0], s->nkbox[0], false);
   cudaEvent_t t0, t1;
   if ((e = cudaEventCreate(&t0)) != cudaSuccess) return e;
@@ -845,11 +862,13 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     }
     const char *pe = std::getenv("CGFD_PRE_EARLY");
     if (pe && pe[0] == '0') s->pre_early = false;
-    // the fault planes inside the interior box, for the PLANE launch when
-    // the interior kernel defers them
+    // the fault planes inside the interior box within the split boxes grown
+    // by 3 nodes, for the PLANE launch when the interior kernel defers them
     for (auto &F : s->faults) {
       const int ii = F.d.i0 - NG;
-      if (ii >= ilo && ii <= ihi) add(6, ii, ii, jlo, jhi, klo, khi);
+      if (ii >= ilo && ii <= ihi && F.nj > 0 && F.nk > 0)
+        add(6, ii, ii, std::max(jlo, F.j0 - 3), std::min(jhi, F.j0 + F.nj + 2), std::max(klo, F.k0 - 3),
+            std::min(khi, F.k0 + F.nk + 2));
     }
     s->pre_overlap = !s->faults.empty();
     const char *po = std::getenv("CGFD_PRE_OVERLAP");
@@ -885,14 +904,16 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
         }
       }
     }
-    // the fault planes deferred to the PLANE launch (welded nodes; the split
-    // nodes belong to the fault kernels)
+    // the fault planes deferred to the PLANE launch (welded nodes of the
+    // grown split box; the split nodes belong to the fault kernels)
     if (s->pre_overlap)
       for (size_t f = 0; f < H.faults.size(); f++) {
+        const FaultState &F = s->faults[f];
         const int i = H.faults[f].i0 - NG;
-        if (i < ilo || i > ihi) continue;
-        for (int k = klo; k <= khi; k++) for (int j = jlo; j <= jhi; j++)
-          if (!(H.faults[f].flag[(size_t)(j + NG) + (size_t)(k + NG) * g.ny] & FL_SPLIT)) nint--;
+        if (i < ilo || i > ihi || F.nj <= 0 || F.nk <= 0) continue;
+        for (int k = std::max(klo, F.k0 - 3); k <= std::min(khi, F.k0 + F.nk + 2); k++)
+          for (int j = std::max(jlo, F.j0 - 3); j <= std::min(jhi, F.j0 + F.nj + 2); j++)
+            if (!(H.faults[f].flag[(size_t)(j + NG) + (size_t)(k + NG) * g.ny] & FL_SPLIT)) nint--;
       }
     s->int_points = nint;
     s->vol_points = nall;

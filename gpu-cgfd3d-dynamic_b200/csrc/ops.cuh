@@ -78,11 +78,14 @@ struct VolArgs {
   real ca, cb;
   int isfree;
   int nfault;
-  // 1: the interior kernel leaves the fault planes x = i0 (welded nodes
-  // too) to a later launch, so that it reads nothing the stage's first
-  // fault kernels write and may run beside them
+  // 1: the interior kernel leaves the fault planes x = i0 within each
+  // fault's split box grown by 3 nodes (welded nodes too; ghost-inclusive
+  // J0, J1, K0, K1 in fdef) to a later launch, so that it reads nothing the
+  // stage's first fault kernels write and may run beside them; outside that
+  // box no tap of a plane point reaches a split node
   int defer_i0;
   int fi0[MAXF];
+  int fdef[MAXF][4];
   const uint8_t *fflag[MAXF];
   PmlFaceDev pml[6];           // indexed 2*dim + side; `on` = 0 when absent
 };

@@ -345,7 +345,9 @@ __global__ void __launch_bounds__(BX * BY, KIND == INTERIOR || KIND == PLANE ? C
   // kernels; with defer_i0 the fault planes go to the PLANE launch
   for (int f = 0; f < a.nfault; f++) {
     const int d = I - a.fi0[f];
-    if (KIND == INTERIOR && d == 0 && a.defer_i0) return;
+    if (KIND == INTERIOR && d == 0 && a.defer_i0 && J >= a.fdef[f][0] && J <= a.fdef[f][1] && K >= a.fdef[f][2] &&
+        K <= a.fdef[f][3])
+      return;
     if (d >= -3 && d <= 3 && (__ldg(a.fflag[f] + J + (long)K * g.ny) & FL_SPLIT)) return;
   }
   const long p = g.at(I, J, K);
