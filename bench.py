@@ -51,9 +51,14 @@ def parse():
                     help="batched form: N seeded scenarios of uneven size advanced as one ensemble, against a "
                          "loop of the plain solver over the same scenarios; prints scenarios/hour")
     ap.add_argument("--e2e-steps", type=int, default=0,
-                    help="steps of the end-to-end run (default: max(--steps, 100), so that the one-time upload "
-                         "is amortised over a run of realistic length)")
+                    help="steps of the end-to-end run (default: the workload's own run length, e.g. the 3000 "
+                         "steps of the 600x300x240 case, so that the one-time upload is amortised as in a real run)")
     return ap.parse_args()
+
+
+# the length of a whole run of each workload (time steps): the end-to-end
+# figure covers one such run, the one-time upload included
+RUN_STEPS = {"hills": 3000, "hills_medium": 3000, "tpv": 600, "large": 4000}
 
 
 def make_problem(workload):
@@ -143,8 +148,10 @@ class ClockSampler:
         load = [r for r in rows if r[5].strip().isdigit() and int(r[5]) >= 50] or rows
         sm = [float(r[2]) for r in load if r[2].strip().replace(".", "").isdigit()]
         mx = [float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit()]
+        pw = [float(r[4]) for r in load if r[4].strip().replace(".", "").isdigit()]
         reasons = sorted({n for r in load for n, v in zip(names, r[7:11]) if v.strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w": statistics.median(pw) if pw else None,
                 "reasons": reasons, "samples": len(rows), "samples_under_load": len(load)}
 
 
@@ -364,13 +371,16 @@ def main():
     # page-locked host memory by cgfd_run_fault_output, in calls of CHUNK
     # steps, stations at the end -- the span of the reference's own timed
     # region (drv_rk_curv_col_allstep)
-    ke = args.e2e_steps or max(args.steps, 100)
+    ke = args.e2e_steps or RUN_STEPS.get(args.workload, max(args.steps, 100))
     chunk = 20
     nbytes_f = 11 * prob.nk * prob.nj * 4 * prob.num_faults
     pinned = torch.empty(chunk * nbytes_f // 4, dtype=torch.float32, pin_memory=True)
+    clk2 = ClockSampler(local)
+    clk2.wait_first_sample()
     barrier(ws)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    t0_wall = time.time()
     s2 = cgfd.Solver(prob, setup=setup)
     t_up = time.perf_counter() - t0
     done = 0
@@ -381,14 +391,16 @@ def main():
     seis = s2.stations()
     torch.cuda.synchronize()
     e2e_s = allmax(ws, time.perf_counter() - t0)
+    e2e_clocks = clk2.stop(t0_wall, time.time())
     s2.close()
     up = setup.upload_bytes
     e2e = {"value": prob.points * ke * ws / e2e_s / 1e9, "unit": unit,
            "h2d_bytes_per_step": int(up / ke), "d2h_bytes_per_step": int(nbytes_f + seis.nbytes / ke),
            "steps": ke, "upload_s": round(t_up, 4), "steps_s": round(e2e_s - t_up, 4),
-           "note": "upload of the prepared problem amortised over the steps; host set-up excluded; the "
-                   "fault fields of every step copied to page-locked host memory by cgfd_run_fault_output "
-                   f"in calls of {chunk} steps"}
+           "ms_per_step": round((e2e_s - t_up) / ke * 1e3, 3), "clocks": e2e_clocks,
+           "note": "the workload's whole run: upload of the prepared problem amortised over its steps; "
+                   "host set-up excluded; the fault fields of every step copied to page-locked host memory by "
+                   f"cgfd_run_fault_output in calls of {chunk} steps"}
 
     line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": run_ms_max / args.steps, "higher_is_better": True,
