@@ -400,7 +400,9 @@ def main():
            "ms_per_step": round((e2e_s - t_up) / ke * 1e3, 3), "clocks": e2e_clocks,
            "note": "the workload's whole run: upload of the prepared problem amortised over its steps; "
                    "host set-up excluded; the fault fields of every step copied to page-locked host memory by "
-                   f"cgfd_run_fault_output in calls of {chunk} steps"}
+                   f"cgfd_run_fault_output in calls of {chunk} steps; a run this long reaches the GPU's power "
+                   "limit (clocks: SM clock and power sampled over this run), so its ms_per_step is the "
+                   "sustained one, the device-timed value above the burst one"}
 
     line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": run_ms_max / args.steps, "higher_is_better": True,
