@@ -18,10 +18,13 @@
 // k_volume<INTERIOR>, whose code holds no boundary logic; slabs that one
 // direction's PML faces reach run k_volume<FACE_X/Y/Z>; PML edges, corners
 // and the bottom ring run k_volume<EDGE>; the four rows under the free
-// surface run k_volume<SHELL>.  Each stage reads the input level (stencil
-// taps come from L1/L2), the metric and the medium once and writes the
-// output levels once; each thread asks L2 early for the lines it reads
-// last (prefetch), and interior threads for the next z row's DRAM misses.
+// surface run k_volume<TOP> away from the PML columns and k_volume<SHELL>
+// in them; the fault planes' welded points next to split nodes run
+// k_volume<PLANE> after the first fault kernels.  Each stage reads the
+// input level (stencil taps come from L1/L2), the metric and the medium
+// once and writes the output levels once; each thread asks L2 early for
+// the lines it reads last (prefetch), and interior threads for the next z
+// row's DRAM misses.
 //
 // A level stores the nine components of a point in two 16-byte groups and
 // one real (Grid::w), so a stencil tap is three loads: x taps are
