@@ -424,7 +424,8 @@ def main():
         line["large"] = large_case(peak, setup_free=setup)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         # as many full steps from the start as fit in about 30 s: the
-        # oracle slows down as the rupture spreads small values over the grid
+        # oracle's steps get slower as the run goes on, so one step would
+        # flatter it
         v, th, sample = oracle_rate(prob, 1000, 0, budget_s=30.0)
         line["cpu_baseline"] = {"value": v, "unit": unit, "cores": th, "kind": "port", "sample": sample}
     if rank == 0:
