@@ -1284,7 +1284,17 @@ int cgfd_ensemble_run(cgfd_ensemble *e, int nsteps) {
       for (int q = 0; q < n; q++) {
         cgfd_solver *s = e->m[q];
         cudaStreamWaitEvent(s->stream, e->fork, 0);
+        // beside the other members each member's step runs best with the y
+        // / z PML slabs on its main stream and the fault slab kernels after
+        // its interior kernel (measured: +2% over the solo default); the
+        // schedules change no arithmetic
+        const int br0 = s->branches;
+        const bool pe0 = s->post_early;
+        if (s->branches == 3) s->branches = 2;
+        s->post_early = false;
         enqueue_step(s, it, nullptr, false);
+        s->branches = br0;
+        s->post_early = pe0;
         cudaEventRecord(e->join[q], s->stream);
         cudaStreamWaitEvent(e->origin, e->join[q], 0);
       }
