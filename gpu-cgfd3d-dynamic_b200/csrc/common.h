@@ -4,9 +4,11 @@
 //
 // HBM layout.  Every 3-D field is stored like the reference's (3 ghost
 // points per side, x fastest, src/forward/gd_t.cu:2124-2140) but with a
-// padded row pitch: index p = (i + XOFF) + j*sy + k*sz for ghost-inclusive
-// indices (i, j, k), sy a multiple of 32 floats.  XOFF = 1 puts the first
-// interior point (i = 3) on a 16-byte boundary.  A wavefield level holds the
+// padded row pitch: index p = (i + xoff) + j*sy + k*sz for ghost-inclusive
+// indices (i, j, k), sy a multiple of 32 points.  xoff (0..7, per grid)
+// puts the first point of the interior box (the first x index after the
+// left PML) on a 128-byte line of the 16-byte component groups, so that a
+// warp's 32 points of one row read exactly four lines.  A wavefield level holds the
 // 9 components (Vx,Vy,Vz,Txx,Tyy,Tzz,Tyz,Txz,Txy) of scmp points as two
 // arrays of 16-byte groups (Vx Vy Vz Txx | Tyy Tzz Tyz Txz) and one of Txy,
 // so that a stencil tap reads all nine with three loads (Grid::w); four levels
@@ -28,7 +30,6 @@
 namespace cgfd {
 
 constexpr int NG = 3;            // ghost points per side
-constexpr int XOFF = 1;          // x offset for 16-byte alignment of interior rows
 constexpr int NCMP = 9;
 constexpr int MAXF = 8;          // faults
 
@@ -82,9 +83,10 @@ enum FaultFlag { FL_SPLIT = 1, FL_RUPY = 2, FL_RUPZ = 4, FL_GRID = 8, FL_T0SET =
 struct Grid {
   int ni, nj, nk;        // interior points
   int nx, ny, nz;        // with ghosts
+  int xoff;              // x offset of the row pitch (see above)
   long sy, sz;           // strides of j and k (elements)
   long scmp;             // elements per component (sz * nz)
-  CGFD_HD long at(int i, int j, int k) const { return (long)(i + XOFF) + (long)j * sy + (long)k * sz; }
+  CGFD_HD long at(int i, int j, int k) const { return (long)(i + xoff) + (long)j * sy + (long)k * sz; }
   // element of component c at point p within one wavefield level: the
   // components 0-3 (Vx Vy Vz Txx) and 4-7 (Tyy Tzz Tyz Txz) are interleaved
   // in 16-byte groups, Txy is stored alone

@@ -119,7 +119,14 @@ int build_setup(const cgfd_config *c, HostSetup &S, std::string &msg) {
   Grid &g = S.g;
   g.ni = c->ni; g.nj = c->nj; g.nk = c->nk;
   g.nx = g.ni + 2*NG; g.ny = g.nj + 2*NG; g.nz = g.nk + 2*NG;
-  g.sy = ((g.nx + XOFF + 31) / 32) * 32;
+  {
+    // the interior box starts after the left x PML (its layers + 1 points)
+    const int ilo = c->pml_layers[0][0] > 0 ? c->pml_layers[0][0] + 1 : 0;
+    // 8 points of 16-byte groups per 128-byte line (the double build's
+    // 32-byte groups need a multiple of 4, which this also is)
+    g.xoff = (8 - (ilo + NG) % 8) % 8;
+  }
+  g.sy = ((g.nx + g.xoff + 31) / 32) * 32;
   g.sz = g.sy * g.ny;
   g.scmp = g.sz * g.nz;
   S.dt = c->dt; S.imethod = c->dynamic_method; S.isfree = c->free_surface ? 1 : 0;
