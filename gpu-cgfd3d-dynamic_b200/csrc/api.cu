@@ -811,10 +811,24 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
       b[0] = i0; b[1] = i1; b[2] = j0; b[3] = j1; b[4] = k0; b[5] = k1;
     };
     const int ni = g.ni, nj = g.nj, nk = g.nk;
-    add(0, ilo, ihi, jlo, jhi, klo, khi);
+    // the interior box is a whole number of 32-point tiles wide in x; the
+    // columns left over (fewer than 32) join the right x PML slab, not a last
+    // tile of each row whose warps would have only those few lanes at work
+    // (unless a fault's neighbourhood reaches them: the fault kernels may
+    // start beside the PML kernels only away from their boxes)
+    int iha = ihi;
+    {
+      const int w = ihi - ilo + 1, wa = w / 32 * 32;
+      const char *at = std::getenv("CGFD_ALIGN_TILES");
+      bool split = wa > 0 && wa < w && !(at && at[0] == '0');
+      for (auto &F : s->faults)
+        if (F.d.i0 - NG + 6 >= ilo + wa && F.d.i0 - NG - 6 <= ihi) split = false;
+      if (split) iha = ilo + wa - 1;
+    }
+    add(0, ilo, iha, jlo, jhi, klo, khi);
     // one PML direction only
     add(2, 0, ilo - 1, jlo, jhi, klo, khi);
-    add(2, ihi + 1, ni - 1, jlo, jhi, klo, khi);
+    add(2, iha + 1, ni - 1, jlo, jhi, klo, khi);
     add(3, ilo, ihi, 0, jlo - 1, klo, khi);
     add(3, ilo, ihi, jhi + 1, nj - 1, klo, khi);
     add(4, ilo, ihi, jlo, jhi, 0, klo - 1);
@@ -866,7 +880,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     // by 3 nodes, for the PLANE launch when the interior kernel defers them
     for (auto &F : s->faults) {
       const int ii = F.d.i0 - NG;
-      if (ii >= ilo && ii <= ihi && F.nj > 0 && F.nk > 0)
+      if (ii >= ilo && ii <= iha && F.nj > 0 && F.nk > 0)
         add(6, ii, ii, std::max(jlo, F.j0 - 3), std::min(jhi, F.j0 + F.nj + 2), std::max(klo, F.k0 - 3),
             std::min(khi, F.k0 + F.nk + 2));
     }
@@ -890,7 +904,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     s->ychunk = std::min(s->ychunk, std::max(1, (jhi - jlo + 8) / 8));
     // points one interior launch / one volume stage updates: the split-node
     // slabs belong to the fault kernels
-    long long nint = (long long)std::max(0, ihi - ilo + 1) * std::max(0, jhi - jlo + 1) * std::max(0, khi - klo + 1);
+    long long nint = (long long)std::max(0, iha - ilo + 1) * std::max(0, jhi - jlo + 1) * std::max(0, khi - klo + 1);
     long long nall = (long long)ni * nj * nk;
     for (size_t f = 0; f < H.faults.size(); f++) {
       const FaultHost &Fh = H.faults[f];
@@ -900,7 +914,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
           const int i = Fh.i0 - NG + d;
           if (i < 0 || i >= ni) continue;
           nall--;
-          if (i >= ilo && i <= ihi && j >= jlo && j <= jhi && k >= klo && k <= khi) nint--;
+          if (i >= ilo && i <= iha && j >= jlo && j <= jhi && k >= klo && k <= khi) nint--;
         }
       }
     }
@@ -910,7 +924,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
       for (size_t f = 0; f < H.faults.size(); f++) {
         const FaultState &F = s->faults[f];
         const int i = H.faults[f].i0 - NG;
-        if (i < ilo || i > ihi || F.nj <= 0 || F.nk <= 0) continue;
+        if (i < ilo || i > iha || F.nj <= 0 || F.nk <= 0) continue;
         for (int k = std::max(klo, F.k0 - 3); k <= std::min(khi, F.k0 + F.nk + 2); k++)
           for (int j = std::max(jlo, F.j0 - 3); j <= std::min(jhi, F.j0 + F.nj + 2); j++)
             if (!(H.faults[f].flag[(size_t)(j + NG) + (size_t)(k + NG) * g.ny] & FL_SPLIT)) nint--;

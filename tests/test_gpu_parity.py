@@ -256,6 +256,34 @@ def test_interior_chunk_choice_changes_nothing(cgfd_lib, monkeypatch):
         assert np.array_equal(g1.wavefield(c), g2.wavefield(c)), WAVE_COMPONENTS[c]
 
 
+def test_interior_whole_tiles(cgfd_lib, monkeypatch):
+    """The interior box is cut to a whole number of 32-point tiles in x and
+    the columns left over join the right x PML slab, whose kernel adds the
+    PML terms only inside the PML layers; with the cut switched off
+    (CGFD_ALIGN_TILES=0) the last tile of each row runs them.  The x
+    direction's sums are formed in the slab kernel's order there, so the two
+    agree to rounding, not bit for bit.  48 points in x with a 5-layer PML:
+    an interior box 36 wide, so 32 + 4 columns, the fault's neighbourhood in
+    the first 32."""
+    p = inputs.tpv_planar(ni=48, nj=80, nk=40, fault_x_index=15, fault_grid=[25, 56, 15, 40], nuc_half=3,
+                          pml=5, nt=20, nsta=4, margin=10)
+    g1 = Solver(p)
+    monkeypatch.setenv("CGFD_ALIGN_TILES", "0")
+    g2 = Solver(p)
+    monkeypatch.delenv("CGFD_ALIGN_TILES")
+    g1.run(17)
+    g2.run(17)
+    assert g1.last_launches() == g2.last_launches()
+    _, _, pts1 = g1.kernel_timing(1)
+    _, _, pts2 = g2.kernel_timing(1)
+    assert pts2 - pts1 == 4 * (80 - 12) * (40 - 6 - 4), (pts1, pts2)
+    for f in ("Vs", "Slip", "Tn", "Ts1"):
+        assert rel_l2(g1.fault(f), g2.fault(f)) <= 1e-6, f
+    for c in range(9):
+        assert rel_l2(g1.wavefield(c), g2.wavefield(c)) <= 1e-6, WAVE_COMPONENTS[c]
+    assert rel_l2(g1.stations(), g2.stations()) <= 1e-6
+
+
 def test_pool_reuse_and_release(cgfd_lib):
     """Solver memory comes from the device's memory pool: a solver made after
     another was destroyed reuses its blocks and runs the same, and the
