@@ -132,7 +132,7 @@ struct cgfd_solver {
   // boxes of each volume kernel kind: 0 interior, 1 generic shell (PML
   // edges / corners, surface rows), 2..4 slabs reached by the PML faces of
   // one direction only (x, y, z)
-  int kbox[8][12][6];
+  int kbox[8][16][6];
   int nkbox[8] = {};
   std::vector<void *> allocs;
   // cgfd_run_fault_output: two device staging buffers of one record (all
@@ -805,8 +805,10 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     auto L = [&](int d, int sd) { return H.pml[d][sd].on ? H.pml[d][sd].L + 1 : 0; };
     const int ilo = L(0, 0), ihi = g.ni - 1 - L(0, 1), jlo = L(1, 0), jhi = g.nj - 1 - L(1, 1);
     const int klo = L(2, 0), khi = s->isfree ? g.nk - 5 : g.nk - 1 - L(2, 1);
+    bool box_overflow = false;
     auto add = [&](int kind, int i0, int i1, int j0, int j1, int k0, int k1) {
       if (i1 < i0 || j1 < j0 || k1 < k0) return;
+      if (s->nkbox[kind] >= 16) { box_overflow = true; return; }
       int *b = s->kbox[kind][s->nkbox[kind]++];
       b[0] = i0; b[1] = i1; b[2] = j0; b[3] = j1; b[4] = k0; b[5] = k1;
     };
@@ -815,7 +817,10 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     // columns left over (fewer than 32) join the right x PML slab, not a last
     // tile of each row whose warps would have only those few lanes at work
     // (unless a fault's neighbourhood reaches them: the fault kernels may
-    // start beside the PML kernels only away from their boxes)
+    // start beside the PML kernels only away from their boxes).  The y and z
+    // PML slabs and the surface rows over the interior box's x extent are
+    // cut the same way, their leftover columns going to the generic edge and
+    // shell kernels
     int iha = ihi;
     {
       const int w = ihi - ilo + 1, wa = w / 32 * 32;
@@ -829,10 +834,14 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     // one PML direction only
     add(2, 0, ilo - 1, jlo, jhi, klo, khi);
     add(2, iha + 1, ni - 1, jlo, jhi, klo, khi);
-    add(3, ilo, ihi, 0, jlo - 1, klo, khi);
-    add(3, ilo, ihi, jhi + 1, nj - 1, klo, khi);
-    add(4, ilo, ihi, jlo, jhi, 0, klo - 1);
-    if (!s->isfree) add(4, ilo, ihi, jlo, jhi, khi + 1, nk - 1);
+    add(3, ilo, iha, 0, jlo - 1, klo, khi);
+    add(3, ilo, iha, jhi + 1, nj - 1, klo, khi);
+    add(4, ilo, iha, jlo, jhi, 0, klo - 1);
+    if (!s->isfree) add(4, ilo, iha, jlo, jhi, khi + 1, nk - 1);
+    add(5, iha + 1, ihi, 0, jlo - 1, klo, khi);
+    add(5, iha + 1, ihi, jhi + 1, nj - 1, klo, khi);
+    add(5, iha + 1, ihi, jlo, jhi, 0, klo - 1);
+    if (!s->isfree) add(5, iha + 1, ihi, jlo, jhi, khi + 1, nk - 1);
     // vertical edges, bottom ring, top ring (edge kernel); surface rows
     // (shell kernel)
     add(5, 0, ilo - 1, 0, jlo - 1, klo, khi);
@@ -846,7 +855,8 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
     const char *tp = std::getenv("CGFD_TOP");
     if (s->isfree && khi + 1 >= klo && !(tp && tp[0] == '0')) {
       // the rows of the PML columns (shell) and the rest (top kernel)
-      add(7, ilo, ihi, jlo, jhi, khi + 1, nk - 1);
+      add(7, ilo, iha, jlo, jhi, khi + 1, nk - 1);
+      add(1, iha + 1, ihi, jlo, jhi, khi + 1, nk - 1);
       add(1, 0, ilo - 1, 0, nj - 1, khi + 1, nk - 1);
       add(1, ihi + 1, ni - 1, 0, nj - 1, khi + 1, nk - 1);
       add(1, ilo, ihi, 0, jlo - 1, khi + 1, nk - 1);
@@ -859,6 +869,7 @@ int cgfd_upload(const cgfd_setup *su, cgfd_solver **out) {
       add(5, ilo, ihi, 0, jlo - 1, khi + 1, nk - 1);
       add(5, ilo, ihi, jhi + 1, nj - 1, khi + 1, nk - 1);
     }
+    if (box_overflow) { destroy(s); return fail(CGFD_ERR_ARG, "too many volume boxes of one kind"); }
     // a stage's first fault kernels read its input at i0-6..i0+6 over the
     // split box grown by 3 nodes: when that region meets no PML slab or edge
     // box for any fault, they may start before those kernels of the

@@ -71,7 +71,7 @@ struct VolArgs {
   Grid g;
   int nbox, nblocks;
   int ychunk;                  // interior kernel: y tiles per chunk (z marches within a chunk)
-  VolBox box[12];
+  VolBox box[16];
   const real *cur, *pre;
   real *out, *end;            // next-stage level (null at the last stage), E
   const real *coef, *free_mat;   // packed metric and medium (coef_row / coef_jac)
